@@ -1,0 +1,331 @@
+"""TEST INFRASTRUCTURE ONLY — the checker, never the product.
+
+ctypes binding for ``oracle/build/liboracle.so`` (the C restatement of the
+FULL-W2V hot path in ``fw2v_oracle.c``) plus a pure-Python restatement of the
+reference's text front end (word reader, vocabulary, global token stream).
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
+import this module.
+
+Reference citations are relative to the tlranda/FULL-W2V repository root.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "build", "liboracle.so")
+UNIGRAM_TABLE_SIZE = 100_000_000
+MAX_STRING = 800
+_lib = None
+
+
+def lib():
+    """Load liboracle.so, building it with make if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            subprocess.run(["make", "-s", "-C", HERE, "build/liboracle.so"], check=True)
+        _lib = C.CDLL(LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+class SamplerCfg(C.Structure):
+    _fields_ = [
+        ("stream", C.c_void_p), ("stream_len", C.c_int64),
+        ("chunk_off", C.c_void_p), ("n_chunks", C.c_int64),
+        ("p_keep", C.c_void_p), ("sample", C.c_float),
+        ("run_start", C.c_void_p), ("run_word", C.c_void_p), ("n_runs", C.c_int64),
+        ("table_size", C.c_int64),
+        ("threads", C.c_int), ("msl", C.c_int), ("negative", C.c_int), ("epochs", C.c_int),
+        ("alpha0", C.c_float), ("train_words", C.c_uint64),
+    ]
+
+
+class StreamState(C.Structure):
+    _fields_ = [("lcg", C.c_uint64), ("wca_own", C.c_uint64), ("alpha", C.c_float)]
+
+
+class TrainCfg(C.Structure):
+    _fields_ = [
+        ("d", C.c_int), ("pitch", C.c_int64), ("window", C.c_int), ("negative", C.c_int),
+        ("sigmoid", C.c_int), ("vec", C.c_int), ("nv", C.c_int), ("exp_table", C.c_void_p),
+    ]
+
+
+def _declare(L):
+    P = C.c_void_p
+    L.orc_lcg_next.restype = C.c_uint64
+    L.orc_lcg_next.argtypes = [C.c_uint64]
+    L.orc_exp_table.argtypes = [P]
+    L.orc_init_syn0.argtypes = [P, C.c_int64, C.c_int, C.c_int64]
+    L.orc_subsample_table.argtypes = [P, C.c_int64, C.c_float, C.c_uint64, P]
+    L.orc_unigram_runs.restype = C.c_int64
+    L.orc_unigram_runs.argtypes = [P, C.c_int64, C.c_int64, P, P, P]
+    L.orc_stream_init.argtypes = [C.POINTER(SamplerCfg), C.c_int, C.POINTER(StreamState)]
+    L.orc_stream_range.argtypes = [C.POINTER(SamplerCfg), C.c_int, C.POINTER(C.c_int64),
+                                   C.POINTER(C.c_int64)]
+    L.orc_sample_epoch.restype = C.c_int
+    L.orc_sample_epoch.argtypes = [C.POINTER(SamplerCfg), C.c_int, C.POINTER(StreamState),
+                                   C.c_int64, P, P, C.c_int64, P, P,
+                                   C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                   C.POINTER(C.c_uint64)]
+    for name in ("orc_train_f32", "orc_train_f64"):
+        f = getattr(L, name)
+        f.restype = C.c_int
+        f.argtypes = [C.POINTER(TrainCfg), P, P, C.c_int64, C.c_int64, P, P, P, P, P]
+    L.orc_heldout_loss.restype = C.c_double
+    L.orc_heldout_loss.argtypes = [P, P, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int64,
+                                   P, P, P, P, C.POINTER(C.c_int64)]
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def lcg_next(r: int) -> int:
+    return int(lib().orc_lcg_next(C.c_uint64(r)))
+
+
+def exp_table() -> np.ndarray:
+    t = np.zeros(1000, np.float32)
+    lib().orc_exp_table(_p(t))
+    return t
+
+
+def init_syn0(V: int, d: int, pitch: int) -> np.ndarray:
+    out = np.zeros((V, pitch), np.float32)
+    lib().orc_init_syn0(_p(out), V, d, pitch)
+    return out
+
+
+def subsample_table(counts: np.ndarray, sample: float, train_words: int) -> np.ndarray:
+    counts = np.ascontiguousarray(counts, np.uint32)
+    out = np.zeros(len(counts), np.float32)
+    lib().orc_subsample_table(_p(counts), len(counts), C.c_float(sample), train_words, _p(out))
+    return out
+
+
+def unigram_runs(counts: np.ndarray, table_size: int = UNIGRAM_TABLE_SIZE, full: bool = False):
+    """Runs (start, word) of the reference unigram table; optionally the full table."""
+    counts = np.ascontiguousarray(counts, np.uint32)
+    V = len(counts)
+    starts = np.zeros(V + 1, np.int64)
+    words = np.zeros(V + 1, np.int32)
+    table = np.zeros(table_size, np.int32) if full else None
+    n = lib().orc_unigram_runs(_p(counts), V, table_size, _p(starts), _p(words),
+                               _p(table) if full else None)
+    starts = starts[: n + 1].copy()
+    words = words[:n].copy()
+    return (starts, words, table) if full else (starts, words)
+
+
+@dataclass
+class Corpus:
+    """Token stream and chunk table as createGlobalStream builds them."""
+    stream: np.ndarray      # int32, trailing 0 included
+    chunk_off: np.ndarray   # int64
+    counts: np.ndarray      # uint32 vocab counts, vocab order
+    words: list = field(default_factory=list)
+    train_words: int = 0
+
+
+@dataclass
+class StreamEpoch:
+    lens: np.ndarray
+    alphas: np.ndarray
+    ids: np.ndarray
+    negs: np.ndarray
+    words_read: int
+
+
+def sample_streams(corpus: Corpus, *, threads: int, msl: int, negative: int, epochs: int,
+                   alpha0: float, sample: float, table_size: int = UNIGRAM_TABLE_SIZE,
+                   runs=None):
+    """Run the reference batch builder for every stream and epoch.
+
+    Returns out[stream][epoch] -> StreamEpoch.
+    """
+    L = lib()
+    stream = np.ascontiguousarray(corpus.stream, np.int32)
+    chunk_off = np.ascontiguousarray(corpus.chunk_off, np.int64)
+    counts = np.ascontiguousarray(corpus.counts, np.uint32)
+    p_keep = subsample_table(counts, sample, corpus.train_words) if sample > 0 else \
+        np.zeros(len(counts), np.float32)
+    if runs is None:
+        runs = unigram_runs(counts, table_size)
+    rs, rw = runs
+    cfg = SamplerCfg(_p(stream).value, len(stream), _p(chunk_off).value, len(chunk_off),
+                     _p(p_keep).value, sample, _p(rs).value, _p(rw).value, len(rw), table_size,
+                     threads, msl, negative, epochs, alpha0, corpus.train_words)
+    out = []
+    for s in range(threads):
+        st = StreamState()
+        L.orc_stream_init(C.byref(cfg), s, C.byref(st))
+        a, b = C.c_int64(), C.c_int64()
+        L.orc_stream_range(C.byref(cfg), s, C.byref(a), C.byref(b))
+        cap = int(chunk_off[b.value] if b.value < len(chunk_off) else len(stream)) - \
+            int(chunk_off[a.value]) + 2
+        per_epoch = []
+        for _ in range(epochs):
+            lens = np.zeros(cap + 2, np.int32)
+            alphas = np.zeros(cap + 2, np.float32)
+            ids = np.zeros(cap + 2, np.int32)
+            negs = np.zeros((cap + 2) * max(negative, 1), np.int32)
+            ne, nk, wr = C.c_int64(), C.c_int64(), C.c_uint64()
+            rc = L.orc_sample_epoch(C.byref(cfg), s, C.byref(st), len(lens), _p(lens),
+                                    _p(alphas), len(ids), _p(ids), _p(negs), C.byref(ne),
+                                    C.byref(nk), C.byref(wr))
+            if rc != 0:
+                raise RuntimeError(f"orc_sample_epoch failed: {rc}")
+            n, k = ne.value, nk.value
+            per_epoch.append(StreamEpoch(lens[:n].copy(), alphas[:n].copy(), ids[:k].copy(),
+                                         negs[: k * negative].copy(), int(wr.value)))
+        out.append(per_epoch)
+    return out
+
+
+def _train_cfg(d, pitch, window, negative, sigmoid, vec, nv, table):
+    return TrainCfg(d, pitch, window, negative, sigmoid, vec, nv, _p(table).value)
+
+
+def train(syn0, syn1neg, lens, alphas, ids, negs, *, d, window, negative, sigmoid="table",
+          precision=32, vec=4, nv=1):
+    """Serial SGNS over the sentences in order; updates syn0/syn1neg in place.
+
+    precision 32: float32 tables, kernel-order arithmetic; 64: float64 tables.
+    """
+    table = exp_table()
+    pitch = syn0.shape[1]
+    cfg = _train_cfg(d, pitch, window, negative, 0 if sigmoid == "table" else 1, vec, nv, table)
+    lens = np.ascontiguousarray(lens, np.int32)
+    starts = np.zeros(len(lens), np.int64)
+    if len(lens) > 1:
+        starts[1:] = np.cumsum(lens[:-1].astype(np.int64))
+    alphas = np.ascontiguousarray(alphas, np.float32)
+    ids = np.ascontiguousarray(ids, np.int32)
+    negs = np.ascontiguousarray(negs, np.int32)
+    if negs.size == 0:
+        negs = np.zeros(1, np.int32)
+    fn = lib().orc_train_f32 if precision == 32 else lib().orc_train_f64
+    want = np.float32 if precision == 32 else np.float64
+    assert syn0.dtype == want and syn1neg.dtype == want
+    assert syn0.flags.c_contiguous and syn1neg.flags.c_contiguous
+    rc = fn(C.byref(cfg), _p(syn0), _p(syn1neg), syn0.shape[0], len(lens), _p(starts),
+            _p(lens), _p(alphas), _p(ids), _p(negs))
+    if rc != 0:
+        raise RuntimeError(f"oracle train failed: {rc}")
+
+
+def heldout_loss(syn0, syn1neg, lens, ids, negs, *, d, window, negative):
+    lens = np.ascontiguousarray(lens, np.int32)
+    starts = np.zeros(len(lens), np.int64)
+    if len(lens) > 1:
+        starts[1:] = np.cumsum(lens[:-1].astype(np.int64))
+    ids = np.ascontiguousarray(ids, np.int32)
+    negs = np.ascontiguousarray(negs, np.int32) if negs.size else np.zeros(1, np.int32)
+    pairs = C.c_int64()
+    tot = lib().orc_heldout_loss(_p(syn0), _p(syn1neg), syn0.shape[1], d, window, negative,
+                                 len(lens), _p(starts), _p(lens), _p(ids), _p(negs),
+                                 C.byref(pairs))
+    return float(tot), int(pairs.value)
+
+
+# ---------------------------------------------------------------------------
+# Text front end (improved_driver_functions.cpp:86-164, 244-281;
+# legacy_driver_functions.cpp:26-95)
+# ---------------------------------------------------------------------------
+
+def read_word(buf: bytes, pos: int):
+    """improved_driver_functions.cpp:86-124 (mmap ReadWord). Returns (word, new_pos)."""
+    n = len(buf)
+    word = bytearray()
+    read = 0
+    while pos < n:
+        read = buf[pos]
+        pos += 1
+        if read == 13:
+            continue
+        if read == 10:
+            if len(word) > 0:
+                pos -= 1
+                break
+            return b"</s>", pos
+        if read == 32 or read == 9:
+            if len(word) > 0:
+                break
+            continue
+        word.append(read)
+        if len(word) >= MAX_STRING - 1:
+            break
+    if pos == n or read in (32, 9, 10):
+        return bytes(word), pos
+    while pos < n and read not in (32, 9, 10):
+        read = buf[pos]
+        pos += 1
+    return bytes(word), pos - 1
+
+
+def learn_vocab(buf: bytes, min_count: int):
+    """LearnVocabFromTrainFile + SortVocab (improved:136-164, legacy:74-95).
+
+    Returns (words, counts, train_words).  The sort is stable (glibc's qsort
+    is a stable merge sort), count descending, </s> pinned at index 0.
+    """
+    index = {b"</s>": 0}
+    words = [b"</s>"]
+    counts = [0]
+    pos, n = 0, len(buf)
+    while pos < n:
+        w, pos = read_word(buf, pos)
+        if pos == n:
+            break
+        i = index.get(w)
+        if i is None:
+            index[w] = len(words)
+            words.append(w)
+            counts.append(1)
+        else:
+            counts[i] += 1
+    order = sorted(range(1, len(words)), key=lambda k: -counts[k])
+    order = [0] + [k for k in order if counts[k] >= min_count]
+    words = [words[k] for k in order]
+    counts = [counts[k] for k in order]
+    train_words = sum(counts) + 1
+    return words, np.array(counts, np.uint32), train_words
+
+
+def create_stream(buf: bytes, words, msl: int, cache_eos: bool):
+    """createGlobalStream (improved:244-281). OOV words are skipped
+    (ReadWordIndex, improved:127-134)."""
+    index = {w: i for i, w in enumerate(words)}
+    stream, chunk_off = [], []
+    sent_length = 0
+    pos, n = 0, len(buf)
+    while pos < n:
+        w = -1
+        while pos < n and w == -1:
+            tok, pos = read_word(buf, pos)
+            w = index.get(tok, -1)
+        if w == -1:
+            break  # OOV run reached EOF; the reference would store -1 here
+        if cache_eos or w != 0:
+            if sent_length == 0:
+                chunk_off.append(len(stream))
+            stream.append(w)
+            sent_length += 1
+            if w == 0 or sent_length >= msl:
+                sent_length = 0
+    stream.append(0)
+    return np.array(stream, np.int32), np.array(chunk_off, np.int64)
+
+
+def corpus_from_text(buf: bytes, *, min_count: int, msl: int, cache_eos: bool) -> Corpus:
+    words, counts, tw = learn_vocab(buf, min_count)
+    stream, chunk_off = create_stream(buf, words, msl, cache_eos)
+    return Corpus(stream, chunk_off, counts, words, tw)
