@@ -1,0 +1,433 @@
+#!/usr/bin/env python3
+"""Benchmark: trained words/sec of SGNS on B200 (one step = one training epoch).
+
+Workload (default): the text-scale corpus — 17M tokens over a 71k vocabulary,
+Zipf(1.0) ranks in a 100-topic mixture with Dirichlet(0.1) weights per
+1000-token sentence, seeded synthetic data — trained with d=128, window=8,
+negative=5, sample=1e-4, alpha=0.025, FP32 tables, on the reference's method.
+"Trained words" counts every token read, subsampled-away ones included, as the
+reference's "Overall Words Per Second" does (FULL-W2V-driver.cu:205, 450).
+
+Own arm (default): the library's epoch loop through its C ABI.
+  value   device time of K epochs (sampler + trainer), inputs resident in HBM,
+          L2 flushed (256 MB write) between epochs and not timed.
+  e2e     the same through the public API from host buffers: every step copies
+          the token stream from pinned host memory (fw2v_load_corpus), trains
+          one epoch and reads the word count back.
+Reference arm (--impl reference): the reference's own program built from its
+sources for sm_100a (oracle/_ref/FULL-W2V) on the same corpus written as text,
+its host threads on all host cores; or, where it cannot run, the CPU
+restatement of its training path (oracle port).
+
+Multi-GPU (torchrun): replicas only — every rank trains its own copy of the job,
+value = words of all ranks / max over ranks of the timed device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "full-w2v_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "trained words/sec"
+UNIT = "words/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            m = json.load(f)
+        return float(m["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, x: float) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(world, x: float) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def default_streams(n_chunks: int) -> int:
+    """Sampling streams (the reference's -threads): enough for the GPU sampler,
+    few enough that each stream's dropped epoch-end partial sentence is a small
+    share of its words (each stream spans >= 256 stored sentences)."""
+    return int(max(1, min(4096, n_chunks // 256)))
+
+
+def cpu_baseline(corpus, cfg, threads, seconds_target=15.0):
+    """The oracle's CPU restatement (sampling + Hogwild FP32 training) on all host
+    cores, on a bounded sample: the first sentences of every stream of one epoch."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    d = cfg["d"]
+    V = len(corpus.counts)
+    ocorp = O.Corpus(corpus.stream, corpus.chunk_off, corpus.counts, [], corpus.train_words)
+    kw = dict(threads=threads, msl=1000, negative=cfg["negative"], epochs=1, alpha0=0.025,
+              sample=cfg["sample"], d=d, window=cfg["window"], n_threads=cores)
+    syn0 = O.init_syn0(V, d, d)
+    syn1 = np.zeros_like(syn0)
+    t0 = time.perf_counter()
+    per = 1
+    wr, wk = O.cpu_sgns(ocorp, syn0, syn1, max_entries_per_stream=per, **kw)
+    dt = time.perf_counter() - t0
+    # grow the sample to ~seconds_target of CPU work
+    per = int(max(1, min(10_000, per * seconds_target / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    wr, wk = O.cpu_sgns(ocorp, syn0, syn1, max_entries_per_stream=per, **kw)
+    dt = time.perf_counter() - t0
+    return {"value": wr / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"first {per} sentences of each of {threads} streams of one epoch "
+                      f"({wr} words read, {wk} kept) in {dt:.1f} s; oracle/fw2v_cpu_sgns.c, "
+                      f"FP32 Hogwild on {cores} threads"}
+
+
+def run_own(args, world, rank, local):
+    import torch
+
+    import fw2v
+    from fw2v import synth
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    corpus, cfg = synth.make_topic_corpus(args.config, n_tokens=args.tokens)
+    T = args.streams or default_streams(len(corpus.chunk_off))
+    d, W, K = cfg["d"], cfg["window"], cfg["negative"]
+    epochs = args.warmup + args.steps
+    conf = fw2v.default_config(layer_size=d, window=W, negative=K, epochs=epochs, threads=T,
+                               msl=1000, alpha=0.025, sample=cfg["sample"],
+                               precision=fw2v.BF16 if args.precision == "bf16" else fw2v.FP32,
+                               device=local)
+    tr = fw2v.Trainer(conf)
+    tr.set_vocab(corpus.counts, corpus.train_words)
+    tr.load_corpus(corpus.stream, corpus.chunk_off)
+    stream = torch.cuda.ExternalStream(tr.stream_handle(), device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    for _ in range(args.warmup):
+        tr.train_epoch()
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stats = []
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(i & 0xFF)
+            starts[i].record(stream)
+            stats.append(tr.train_epoch())
+            ends[i].record(stream)
+        torch.cuda.synchronize(dev)
+    barrier(world)
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_s = max_over_ranks(world, sum(step_ms) / 1e3)
+    words = sum(s.words_read for s in stats)
+    kept = sum(s.words_kept for s in stats)
+    words_all = sum_over_ranks(world, float(words))
+    value = words_all / total_s
+    train_ms = float(np.mean([s.train_ms for s in stats]))
+    sampler_ms = float(np.mean([s.sampler_ms for s in stats]))
+
+    # e2e: host buffers through the public API every step
+    pinned = torch.empty(len(corpus.stream), dtype=torch.int32, pin_memory=True)
+    pinned.numpy()[:] = corpus.stream
+    host_stream = pinned.numpy()
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_words = 0
+    e2e_s = 0.0
+    for i in range(e2e_steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(i & 0xFF)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        tr.load_corpus(host_stream, corpus.chunk_off)
+        st = tr.train_epoch()
+        e2e_words += st.words_read
+        e2e_s += time.perf_counter() - t0
+    e2e_s = max_over_ranks(world, e2e_s)
+    e2e_value = sum_over_ranks(world, float(e2e_words)) / e2e_s
+    h2d = corpus.stream.nbytes + corpus.chunk_off.nbytes
+    d2h = T * 8 + 4
+
+    hbm, peak_kind = peaks()
+    kept_per_epoch = kept / args.steps
+    bytes_per_launch = kept_per_epoch * (2 * d * 4 * (K + 2) + 4 * (1 + K))
+    achieved = bytes_per_launch / (train_ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tr_map = json.load(f)
+        key = f"{args.config}:{args.tokens or cfg['n_tokens']}:{args.precision}"
+        if key in tr_map:
+            traffic = tr_map[key]["dram_bytes_per_launch"]
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if args.precision == "fp32" else "bf16-tables/f32-math",
+        "data": "synthetic (seeded topic-mixture corpus, generated in-process)",
+        "config": {"workload": f"{args.config}: {cfg['n_tokens']/1e6:.0f}M-token topic corpus, "
+                               f"V={len(corpus.counts)}, d={d}, window={W}, negative={K}, "
+                               f"sample={cfg['sample']}, msl=1000, {T} sampling streams, "
+                               f"{args.precision} tables",
+                   "tokens_per_epoch": int(len(corpus.stream) - 1), "vocab": len(corpus.counts),
+                   "layer_size": d, "window": W, "negative": K, "streams": T,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "flushed between steps (256 MB write, untimed)"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
+        "gpu_launches": 3 * args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": traffic,
+                     "kernel": "sgns_train_kernel", "peak_kind": peak_kind,
+                     "bytes_per_launch": bytes_per_launch, "launch_ms": train_ms},
+        "breakdown": {"sampler_ms": sampler_ms, "train_ms": train_ms,
+                      "kept_fraction": kept / max(words, 1)},
+    }
+    clocks = clk.summary()
+    if clocks:
+        out["clocks"] = clocks
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(corpus, cfg, T)
+    tr.close()
+    return out
+
+
+def run_reference(args, world, rank):
+    """The reference program (oracle/_ref/FULL-W2V) on the same corpus, or the
+    CPU port where it cannot run."""
+    from fw2v import synth
+    from oracle import oracle as O
+
+    if world > 1 and rank != 0:
+        return None
+    corpus, cfg = synth.make_topic_corpus(args.config, n_tokens=args.tokens)
+    T_stream = args.streams or default_streams(len(corpus.chunk_off))
+    cores = os.cpu_count() or 1
+    binary = os.path.join(ROOT, "oracle", "_ref", "FULL-W2V")
+    reason = None
+    if cfg["d"] > 256 or cfg["d"] % 32:
+        reason = f"reference kernel unsupported at d={cfg['d']} (shared-memory overlap / partial warp)"
+    elif not os.path.exists(binary):
+        reason = "oracle/_ref/FULL-W2V not built"
+    if reason is None:
+        res = reference_program(args, corpus, cfg, binary, cores)
+        if isinstance(res, dict):
+            return res
+        reason = res
+    base = cpu_baseline(corpus, cfg, T_stream)
+    base["sample"] += f"; reference program not run: {reason}"
+    return {"metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": args.config}, "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def reference_program(args, corpus, cfg, binary, cores):
+    """Run FULL-W2V with thread/stream/batch settings under which every launch
+    reads only buffers it has filled: each host thread must complete >= S full
+    batches before its final launch (FULL-W2V-driver.cu:305-318 launches all
+    kernel-batch-size blocks and reuses the buffers of stream S-1 otherwise
+    unfilled).  Sentence counts per thread come from the oracle's restatement of
+    the reference batch builder."""
+    from fw2v import synth
+    from oracle import oracle as O
+
+    raw_text = synth_text(args, cfg)
+    if raw_text is None:
+        return "could not write the corpus as text"
+    epochs = args.steps
+    batch, streams = 200, 4
+    ocorp = O.Corpus(corpus.stream, corpus.chunk_off, corpus.counts, [], corpus.train_words)
+    threads = min(cores, len(corpus.chunk_off))
+    while threads >= 1:
+        per = O.sample_streams(ocorp, threads=threads, msl=1000, negative=cfg["negative"],
+                               epochs=1, alpha0=0.025, sample=cfg["sample"])
+        min_entries = min(len(p[0].lens) for p in per) * epochs
+        if min_entries >= streams * batch + 1:
+            break
+        threads //= 2
+    if threads < 1:
+        return "corpus too small for the reference's launch pattern"
+    cmd = [binary, "-train", raw_text, "-size", str(cfg["d"]), "-window", str(cfg["window"]),
+           "-negative", str(cfg["negative"]), "-sample", str(cfg["sample"]), "-iter", str(epochs),
+           "-alpha", "0.025", "-min-count", str(cfg["min_count"]), "-threads", str(threads),
+           "-streams", str(streams), "-kernel-batch-size", str(batch), "-msl", "1000",
+           "-debug", "0", "-no-export", "-output", os.devnull]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    finally:
+        shutil.rmtree(os.path.dirname(raw_text), ignore_errors=True)
+    if r.returncode != 0:
+        return f"reference exited {r.returncode}: {r.stderr[-300:]}"
+    wps = [ln for ln in r.stdout.splitlines() if ln.startswith("Overall Words Per Second:")]
+    tim = [ln for ln in r.stdout.splitlines() if ln.startswith("Overall time:")]
+    if not wps:
+        return "no words/sec line from the reference"
+    value = float(wps[0].split(":")[1])
+    secs = float(tim[0].split(":")[1]) if tim else None
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": epochs,
+            "warmup": 0, "ms_per_step": secs * 1e3 / epochs if secs else None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (same seeded corpus, written as text)", "impl": "reference",
+            "config": {"workload": f"{args.config} as text, reference FULL-W2V sm_100a",
+                       "threads": threads, "streams": streams, "kernel_batch_size": batch},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"{epochs} epochs of the full corpus; the reference's "
+                                       f"host threads on {threads} cores feed its sm_100a kernel"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def synth_text(args, cfg):
+    from fw2v import synth
+    n = args.tokens or cfg["n_tokens"]
+    seed = 1234 + int(args.config[1:])
+    raw, _ = synth.topic_tokens(n, cfg["vocab"], cfg["topics"], cfg["zipf_s"], seed=seed)
+    ends = np.arange(1000, len(raw) + 1000, 1000)
+    ends[-1] = len(raw)
+    tmp = tempfile.mkdtemp(prefix="fw2v_ref_")
+    path = os.path.join(tmp, "corpus.txt")
+    with open(path, "wb") as f:
+        s = 0
+        for e in ends:
+            f.write((" ".join(f"w{t}" for t in raw[s:e]) + "\n").encode())
+            s = e
+    return path
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fw2v", choices=["fw2v", "reference"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--tokens", type=int, default=None, help="override the corpus size")
+    ap.add_argument("--streams", type=int, default=None, help="sampling streams (-threads)")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        out = run_reference(args, world, rank)
+    else:
+        out = run_own(args, world, rank, local)
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

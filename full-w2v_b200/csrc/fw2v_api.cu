@@ -1,0 +1,622 @@
+// C ABI of libfw2v (include/fw2v.h): handle lifetime, device memory, and the
+// epoch loop of Train_SGNS (FULL-W2V-driver.cu:80-354) as two kernel launches
+// per epoch (sampler, trainer) with no host work in between.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/fw2v.h"
+#include "fw2v_common.cuh"
+
+extern "C" void fw2v_exp_table(float* t);
+extern "C" int fw2v_unigram_firsts(const uint32_t* counts, int64_t V, int64_t size, int64_t* firsts);
+
+namespace fw2v {
+cudaError_t launch_sampler(const SamplerParams& p, int64_t* entry_prefix, cudaStream_t st);
+cudaError_t launch_train(const TrainParams& p, int num_sms, cudaStream_t st);
+cudaError_t launch_heldout(const TrainParams& p, double* loss, unsigned long long* pairs, cudaStream_t st);
+cudaError_t launch_init_tables(float* syn0, int64_t V, int d, int64_t pitch, const uint32_t* d_counts,
+                               float sample, uint64_t train_words, float* p_keep, const int64_t* d_firsts,
+                               int n_firsts, int32_t* unigram, int64_t table_size, cudaStream_t st);
+size_t train_smem_bytes(int window, int64_t pitch, int warps);
+cudaError_t launch_validate_ids(const int32_t* ids, int64_t n, int64_t vocab, int* flag, cudaStream_t st);
+}  // namespace fw2v
+
+using namespace fw2v;
+
+struct fw2v_handle {
+  fw2v_config cfg{};
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  std::string err;
+
+  int64_t V = 0;
+  uint64_t train_words = 0;
+  int64_t pitch = 0;
+  float* syn0 = nullptr;
+  float* syn1neg = nullptr;
+  float* p_keep = nullptr;
+  int32_t* unigram = nullptr;
+  float* exp_table = nullptr;
+
+  int32_t* stream_ids = nullptr;
+  int64_t stream_len = 0;
+  int64_t* chunk_off = nullptr;
+  int64_t n_chunks = 0;
+
+  uint64_t* lcg = nullptr;
+  uint64_t* wca = nullptr;
+  float* alpha = nullptr;
+  int64_t* ent_start = nullptr;
+  int32_t* ent_len = nullptr;
+  float* ent_alpha = nullptr;
+  int32_t* kept_ids = nullptr;
+  int32_t* kept_negs = nullptr;
+  int64_t* n_entries = nullptr;
+  int64_t* n_kept = nullptr;
+  uint64_t* words = nullptr;
+  int64_t* entry_prefix = nullptr;
+
+  int* error_flag = nullptr;
+  unsigned long long* work_counter = nullptr;
+
+  bool sampled = false;
+  int epochs_done = 0;
+  uint64_t words_total = 0;
+};
+
+namespace {
+
+fw2v_status fail(fw2v_handle* h, fw2v_status s, const char* fmt, ...) {
+  if (h) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    h->err = buf;
+  }
+  return s;
+}
+
+#define CK(h, call)                                                                         \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess) {                                                                \
+      return fail((h), e_ == cudaErrorMemoryAllocation ? FW2V_ERR_NOMEM : FW2V_ERR_CUDA,    \
+                  "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);    \
+    }                                                                                       \
+  } while (0)
+
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+template <typename T>
+cudaError_t dalloc(T*& p, size_t n) {
+  dfree(p);
+  return cudaMalloc((void**)&p, std::max<size_t>(n, 1) * sizeof(T));
+}
+
+int64_t pitch_for(int d) { return ((int64_t)d + 7) / 8 * 8; }
+
+fw2v_status check_flag(fw2v_handle* h, const char* what) {
+  int flag = 0;
+  CK(h, cudaMemcpyAsync(&flag, h->error_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  if (flag) {
+    CK(h, cudaMemsetAsync(h->error_flag, 0, sizeof(int), h->stream));
+    return fail(h, FW2V_ERR_BOUNDS, "%s: an id outside [0, V) or a read past the token stream", what);
+  }
+  return FW2V_OK;
+}
+
+TrainParams base_train_params(fw2v_handle* h) {
+  TrainParams p{};
+  p.syn0 = h->syn0;
+  p.syn1neg = h->syn1neg;
+  p.pitch = h->pitch;
+  p.vocab = h->V;
+  p.d = h->cfg.layer_size;
+  p.window = h->cfg.window;
+  p.negative = h->cfg.negative;
+  p.sigmoid = h->cfg.sigmoid;
+  p.deterministic = h->cfg.deterministic;
+  p.error_flag = h->error_flag;
+  p.work_counter = h->work_counter;
+  p.exp_table = h->exp_table;
+  return p;
+}
+
+}  // namespace
+
+extern "C" {
+
+void fw2v_config_default(fw2v_config* c) {
+  std::memset(c, 0, sizeof(*c));
+  c->layer_size = 100;
+  c->window = 5;
+  c->negative = 5;
+  c->epochs = 5;
+  c->threads = 12;
+  c->msl = 1000;
+  c->alpha = 0.025f;
+  c->sample = 1e-3f;
+  c->sigmoid = FW2V_SIGMOID_TABLE;
+  c->precision = FW2V_FP32;
+  c->deterministic = 0;
+  c->device = 0;
+}
+
+void fw2v_lane_layout(int32_t layer_size, int32_t precision, int32_t* vec, int32_t* nv, int64_t* pitch) {
+  (void)precision;
+  const int64_t P = pitch_for(layer_size);
+  if (P <= 64) {
+    *vec = 2;
+    *nv = 1;
+  } else {
+    *vec = 4;
+    const int n = (int)((P + 127) / 128);
+    *nv = n <= 4 ? n : (n <= 6 ? 6 : 8);
+  }
+  *pitch = P;
+}
+
+const char* fw2v_status_string(fw2v_status s) {
+  switch (s) {
+    case FW2V_OK: return "ok";
+    case FW2V_ERR_ARGUMENT: return "invalid argument";
+    case FW2V_ERR_CUDA: return "CUDA error";
+    case FW2V_ERR_NOMEM: return "out of memory";
+    case FW2V_ERR_STATE: return "call out of order";
+    case FW2V_ERR_BOUNDS: return "id out of range";
+    case FW2V_ERR_NO_DEVICE: return "no usable CUDA device";
+  }
+  return "unknown status";
+}
+
+const char* fw2v_last_error(fw2v_handle* h) { return h ? h->err.c_str() : ""; }
+
+const char* fw2v_version(void) { return "fw2v 1.0 sm_100a"; }
+
+void* fw2v_stream(fw2v_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+fw2v_status fw2v_create(const fw2v_config* cfg, fw2v_handle** out) {
+  if (!cfg || !out) return FW2V_ERR_ARGUMENT;
+  *out = nullptr;
+  const fw2v_config& c = *cfg;
+  if (c.layer_size < 1 || c.layer_size > 1024 || c.window < 1 || c.window > kMaxWindow ||
+      c.negative < 0 || c.negative > kMaxNegative || c.epochs < 0 || c.threads < 1 || c.msl < 1 ||
+      !(c.alpha > 0) || !(c.sample >= 0) || (c.sigmoid != 0 && c.sigmoid != 1) ||
+      (c.precision != FW2V_FP32 && c.precision != FW2V_BF16))
+    return FW2V_ERR_ARGUMENT;
+  if (c.precision == FW2V_BF16) return FW2V_ERR_ARGUMENT;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= c.device || c.device < 0) return FW2V_ERR_NO_DEVICE;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, c.device) != cudaSuccess || prop.major != 10) return FW2V_ERR_NO_DEVICE;
+  if (cudaSetDevice(c.device) != cudaSuccess) return FW2V_ERR_NO_DEVICE;
+  const int64_t P = pitch_for(c.layer_size);
+  if (train_smem_bytes(c.window, P, 1) > (size_t)prop.sharedMemPerBlockOptin) return FW2V_ERR_ARGUMENT;
+  fw2v_handle* h = new fw2v_handle();
+  h->cfg = c;
+  h->num_sms = prop.multiProcessorCount;
+  h->pitch = P;
+  auto cleanup = [&](fw2v_status s) {
+    fw2v_destroy(h);
+    return s;
+  };
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return cleanup(FW2V_ERR_CUDA);
+  for (auto& e : h->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return cleanup(FW2V_ERR_CUDA);
+  if (dalloc(h->error_flag, 1) != cudaSuccess || dalloc(h->work_counter, 1) != cudaSuccess ||
+      dalloc(h->exp_table, kExpTableSize) != cudaSuccess)
+    return cleanup(FW2V_ERR_NOMEM);
+  float table[kExpTableSize];
+  fw2v_exp_table(table);
+  if (cudaMemcpy(h->exp_table, table, sizeof(table), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(h->error_flag, 0, sizeof(int)) != cudaSuccess)
+    return cleanup(FW2V_ERR_CUDA);
+  *out = h;
+  return FW2V_OK;
+}
+
+void fw2v_destroy(fw2v_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->cfg.device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  dfree(h->syn0); dfree(h->syn1neg); dfree(h->p_keep); dfree(h->unigram); dfree(h->exp_table);
+  dfree(h->stream_ids); dfree(h->chunk_off);
+  dfree(h->lcg); dfree(h->wca); dfree(h->alpha);
+  dfree(h->ent_start); dfree(h->ent_len); dfree(h->ent_alpha);
+  dfree(h->kept_ids); dfree(h->kept_negs);
+  dfree(h->n_entries); dfree(h->n_kept); dfree(h->words); dfree(h->entry_prefix);
+  dfree(h->error_flag); dfree(h->work_counter);
+  for (auto& e : h->ev)
+    if (e) cudaEventDestroy(e);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+fw2v_status fw2v_set_vocab(fw2v_handle* h, const uint32_t* counts, int64_t V, uint64_t train_words) {
+  if (!h || !counts || V < 2 || V > (int64_t)INT32_MAX) return fail(h, FW2V_ERR_ARGUMENT, "set_vocab: V >= 2 required");
+  CK(h, cudaSetDevice(h->cfg.device));
+  const int d = h->cfg.layer_size;
+  const int64_t P = h->pitch;
+  h->V = V;
+  h->train_words = train_words;
+  CK(h, dalloc(h->syn0, (size_t)V * P));
+  CK(h, dalloc(h->syn1neg, (size_t)V * P));
+  CK(h, dalloc(h->p_keep, V));
+  CK(h, dalloc(h->unigram, kUnigramTableSize));
+  CK(h, cudaMemsetAsync(h->syn0, 0, (size_t)V * P * sizeof(float), h->stream));
+  CK(h, cudaMemsetAsync(h->syn1neg, 0, (size_t)V * P * sizeof(float), h->stream));
+  std::vector<int64_t> firsts((size_t)V - 1);
+  fw2v_unigram_firsts(counts, V, kUnigramTableSize, firsts.data());
+  uint32_t* d_counts = nullptr;
+  int64_t* d_firsts = nullptr;
+  CK(h, dalloc(d_counts, V));
+  CK(h, dalloc(d_firsts, V - 1));
+  CK(h, cudaMemcpyAsync(d_counts, counts, V * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(d_firsts, firsts.data(), (V - 1) * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
+  CK(h, launch_init_tables(h->syn0, V, d, P, d_counts, h->cfg.sample, train_words, h->p_keep, d_firsts,
+                           (int)(V - 1), h->unigram, kUnigramTableSize, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  dfree(d_counts);
+  dfree(d_firsts);
+  h->sampled = false;
+  return FW2V_OK;
+}
+
+fw2v_status fw2v_load_corpus(fw2v_handle* h, const int32_t* stream, int64_t stream_len, const int64_t* chunk_off,
+                             int64_t n_chunks) {
+  if (!h || !stream || !chunk_off || stream_len < 1 || n_chunks < 1)
+    return fail(h, FW2V_ERR_ARGUMENT, "load_corpus: empty corpus");
+  if (h->V == 0) return fail(h, FW2V_ERR_STATE, "load_corpus before set_vocab");
+  if (h->cfg.threads > n_chunks)
+    return fail(h, FW2V_ERR_ARGUMENT, "load_corpus: threads (%d) > sentence chunks (%lld)", h->cfg.threads,
+                (long long)n_chunks);
+  if (stream[stream_len - 1] != 0) return fail(h, FW2V_ERR_ARGUMENT, "load_corpus: stream must end with 0");
+  for (int64_t i = 0; i < n_chunks; i++) {
+    if (chunk_off[i] < 0 || chunk_off[i] >= stream_len || (i > 0 && chunk_off[i] < chunk_off[i - 1]))
+      return fail(h, FW2V_ERR_ARGUMENT, "load_corpus: chunk offset %lld invalid", (long long)i);
+  }
+  CK(h, cudaSetDevice(h->cfg.device));
+  const int T = h->cfg.threads;
+  const int K = h->cfg.negative;
+  if (stream_len != h->stream_len || n_chunks != h->n_chunks || !h->stream_ids) {
+    CK(h, dalloc(h->stream_ids, stream_len));
+    CK(h, dalloc(h->chunk_off, n_chunks));
+    CK(h, dalloc(h->kept_ids, stream_len));
+    CK(h, dalloc(h->kept_negs, (size_t)stream_len * std::max(K, 1)));
+    CK(h, dalloc(h->ent_start, stream_len + 2 * (int64_t)T));
+    CK(h, dalloc(h->ent_len, stream_len + 2 * (int64_t)T));
+    CK(h, dalloc(h->ent_alpha, stream_len + 2 * (int64_t)T));
+    CK(h, dalloc(h->lcg, T));
+    CK(h, dalloc(h->wca, T));
+    CK(h, dalloc(h->alpha, T));
+    CK(h, dalloc(h->n_entries, T));
+    CK(h, dalloc(h->n_kept, T));
+    CK(h, dalloc(h->words, T));
+    CK(h, dalloc(h->entry_prefix, T + 1));
+  }
+  h->stream_len = stream_len;
+  h->n_chunks = n_chunks;
+  CK(h, cudaMemcpyAsync(h->stream_ids, stream, stream_len * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(h->chunk_off, chunk_off, n_chunks * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
+  CK(h, launch_validate_ids(h->stream_ids, stream_len, h->V, h->error_flag, h->stream));
+  // Stream state (FULL-W2V-driver.cu:113-114): LCG seeded with the id, alpha0.
+  std::vector<uint64_t> lcg(T), zero(T, 0);
+  std::vector<float> alpha(T, h->cfg.alpha);
+  for (int s = 0; s < T; s++) lcg[s] = (uint64_t)s;
+  CK(h, cudaMemcpyAsync(h->lcg, lcg.data(), T * sizeof(uint64_t), cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(h->wca, zero.data(), T * sizeof(uint64_t), cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(h->alpha, alpha.data(), T * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+  fw2v_status s = check_flag(h, "load_corpus");
+  if (s != FW2V_OK) return s;
+  h->sampled = false;
+  h->epochs_done = 0;
+  h->words_total = 0;
+  return FW2V_OK;
+}
+
+fw2v_status fw2v_sample_epoch(fw2v_handle* h) {
+  if (!h) return FW2V_ERR_ARGUMENT;
+  if (!h->stream_ids || h->V == 0) return fail(h, FW2V_ERR_STATE, "sample_epoch before load_corpus");
+  CK(h, cudaSetDevice(h->cfg.device));
+  SamplerParams p{};
+  p.stream = h->stream_ids;
+  p.stream_len = h->stream_len;
+  p.chunk_off = h->chunk_off;
+  p.n_chunks = h->n_chunks;
+  p.p_keep = h->p_keep;
+  p.sample = h->cfg.sample;
+  p.unigram = h->unigram;
+  p.table_size = kUnigramTableSize;
+  p.threads = h->cfg.threads;
+  p.msl = h->cfg.msl;
+  p.negative = h->cfg.negative;
+  p.epochs = h->cfg.epochs;
+  p.alpha0 = h->cfg.alpha;
+  p.train_words = h->train_words;
+  p.lcg = h->lcg;
+  p.wca_own = h->wca;
+  p.alpha = h->alpha;
+  p.ent_start = h->ent_start;
+  p.ent_len = h->ent_len;
+  p.ent_alpha = h->ent_alpha;
+  p.kept_ids = h->kept_ids;
+  p.kept_negs = h->kept_negs;
+  p.n_entries = h->n_entries;
+  p.n_kept = h->n_kept;
+  p.words = h->words;
+  p.error_flag = h->error_flag;
+  CK(h, cudaEventRecord(h->ev[0], h->stream));
+  CK(h, launch_sampler(p, h->entry_prefix, h->stream));
+  CK(h, cudaEventRecord(h->ev[1], h->stream));
+  h->sampled = true;
+  return FW2V_OK;
+}
+
+fw2v_status fw2v_epoch_sample_sizes(fw2v_handle* h, int64_t* n_entries, int64_t* n_kept) {
+  if (!h || !h->sampled) return fail(h, FW2V_ERR_STATE, "no sampled epoch");
+  const int T = h->cfg.threads;
+  std::vector<int64_t> ne(T), nk(T);
+  CK(h, cudaMemcpyAsync(ne.data(), h->n_entries, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaMemcpyAsync(nk.data(), h->n_kept, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+  fw2v_status s = check_flag(h, "sample_epoch");
+  if (s != FW2V_OK) return s;
+  int64_t a = 0, b = 0;
+  for (int i = 0; i < T; i++) {
+    a += ne[i];
+    b += nk[i];
+  }
+  if (n_entries) *n_entries = a;
+  if (n_kept) *n_kept = b;
+  return FW2V_OK;
+}
+
+fw2v_status fw2v_epoch_samples(fw2v_handle* h, int32_t* lens, float* alphas, int32_t* ids, int32_t* negs,
+                               int64_t* entries_per_stream, int64_t* kept_per_stream, uint64_t* words_per_stream) {
+  if (!h || !h->sampled) return fail(h, FW2V_ERR_STATE, "no sampled epoch");
+  const int T = h->cfg.threads;
+  const int K = h->cfg.negative;
+  std::vector<int64_t> ne(T), nk(T);
+  std::vector<uint64_t> wr(T);
+  std::vector<int64_t> off(h->n_chunks);
+  CK(h, cudaMemcpyAsync(ne.data(), h->n_entries, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaMemcpyAsync(nk.data(), h->n_kept, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaMemcpyAsync(wr.data(), h->words, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaMemcpyAsync(off.data(), h->chunk_off, h->n_chunks * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+  fw2v_status st = check_flag(h, "sample_epoch");
+  if (st != FW2V_OK) return st;
+  int64_t eo = 0, ko = 0;
+  for (int s = 0; s < T; s++) {
+    int64_t first, end;
+    stream_range(h->n_chunks, T, s, &first, &end);
+    const int64_t kb = off[first];
+    const int64_t eb = kb + 2 * (int64_t)s;
+    if (lens) CK(h, cudaMemcpyAsync(lens + eo, h->ent_len + eb, ne[s] * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    if (alphas) CK(h, cudaMemcpyAsync(alphas + eo, h->ent_alpha + eb, ne[s] * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    if (ids) CK(h, cudaMemcpyAsync(ids + ko, h->kept_ids + kb, nk[s] * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    if (negs && K > 0)
+      CK(h, cudaMemcpyAsync(negs + ko * K, h->kept_negs + kb * K, nk[s] * K * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    if (entries_per_stream) entries_per_stream[s] = ne[s];
+    if (kept_per_stream) kept_per_stream[s] = nk[s];
+    if (words_per_stream) words_per_stream[s] = wr[s];
+    eo += ne[s];
+    ko += nk[s];
+  }
+  CK(h, cudaStreamSynchronize(h->stream));
+  return FW2V_OK;
+}
+
+fw2v_status fw2v_train_sampled(fw2v_handle* h, fw2v_epoch_stats* stats) {
+  if (!h || !h->sampled) return fail(h, FW2V_ERR_STATE, "train_sampled without a sampled epoch");
+  CK(h, cudaSetDevice(h->cfg.device));
+  TrainParams p = base_train_params(h);
+  p.ids = h->kept_ids;
+  p.negs = h->kept_negs;
+  p.source = kSourceEpoch;
+  p.entry_prefix = h->entry_prefix;
+  p.chunk_off = h->chunk_off;
+  p.n_chunks = h->n_chunks;
+  p.threads = h->cfg.threads;
+  p.ent_start = h->ent_start;
+  p.ent_len = h->ent_len;
+  p.ent_alpha = h->ent_alpha;
+  CK(h, cudaMemsetAsync(h->work_counter, 0, sizeof(unsigned long long), h->stream));
+  CK(h, launch_train(p, h->num_sms, h->stream));
+  CK(h, cudaEventRecord(h->ev[2], h->stream));
+  const int T = h->cfg.threads;
+  std::vector<uint64_t> wr(T);
+  std::vector<int64_t> ne(T), nk(T);
+  CK(h, cudaMemcpyAsync(wr.data(), h->words, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+  if (stats) {
+    CK(h, cudaMemcpyAsync(ne.data(), h->n_entries, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaMemcpyAsync(nk.data(), h->n_kept, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+  }
+  fw2v_status s = check_flag(h, "train");
+  if (s != FW2V_OK) return s;
+  uint64_t words = 0;
+  for (int i = 0; i < T; i++) words += wr[i];
+  h->words_total += words;
+  h->epochs_done++;
+  h->sampled = false;
+  if (stats) {
+    stats->words_read = words;
+    stats->words_kept = 0;
+    stats->sentences = 0;
+    for (int i = 0; i < T; i++) {
+      stats->words_kept += (uint64_t)nk[i];
+      stats->sentences += (uint64_t)ne[i];
+    }
+    CK(h, cudaEventElapsedTime(&stats->sampler_ms, h->ev[0], h->ev[1]));
+    CK(h, cudaEventElapsedTime(&stats->train_ms, h->ev[1], h->ev[2]));
+  }
+  return FW2V_OK;
+}
+
+fw2v_status fw2v_train_epoch(fw2v_handle* h, fw2v_epoch_stats* stats) {
+  fw2v_status s = fw2v_sample_epoch(h);
+  if (s != FW2V_OK) return s;
+  return fw2v_train_sampled(h, stats);
+}
+
+fw2v_status fw2v_train(fw2v_handle* h, uint64_t* words_read) {
+  if (!h) return FW2V_ERR_ARGUMENT;
+  uint64_t before = h->words_total;
+  while (h->epochs_done < h->cfg.epochs) {
+    fw2v_status s = fw2v_train_epoch(h, nullptr);
+    if (s != FW2V_OK) return s;
+  }
+  if (words_read) *words_read = h->words_total - before;
+  return FW2V_OK;
+}
+
+fw2v_status fw2v_words_trained(fw2v_handle* h, uint64_t* words) {
+  if (!h || !words) return FW2V_ERR_ARGUMENT;
+  *words = h->words_total;
+  return FW2V_OK;
+}
+
+static fw2v_status copy_table(fw2v_handle* h, float* dst, const float* src, int64_t stride, bool to_host) {
+  if (!h || !dst || stride < h->cfg.layer_size) return fail(h, FW2V_ERR_ARGUMENT, "table copy: bad stride");
+  if (h->V == 0) return fail(h, FW2V_ERR_STATE, "tables not allocated");
+  CK(h, cudaSetDevice(h->cfg.device));
+  const size_t w = (size_t)h->cfg.layer_size * sizeof(float);
+  if (to_host) {
+    CK(h, cudaMemcpy2DAsync(dst, stride * sizeof(float), src, h->pitch * sizeof(float), w, h->V,
+                            cudaMemcpyDeviceToHost, h->stream));
+  } else {
+    CK(h, cudaMemcpy2DAsync(dst, h->pitch * sizeof(float), src, stride * sizeof(float), w, h->V,
+                            cudaMemcpyHostToDevice, h->stream));
+  }
+  CK(h, cudaStreamSynchronize(h->stream));
+  return FW2V_OK;
+}
+
+fw2v_status fw2v_get_syn0(fw2v_handle* h, float* out, int64_t row_stride) {
+  return copy_table(h, out, h ? h->syn0 : nullptr, row_stride, true);
+}
+fw2v_status fw2v_get_syn1neg(fw2v_handle* h, float* out, int64_t row_stride) {
+  return copy_table(h, out, h ? h->syn1neg : nullptr, row_stride, true);
+}
+fw2v_status fw2v_set_tables(fw2v_handle* h, const float* syn0, const float* syn1neg, int64_t row_stride) {
+  fw2v_status s = FW2V_OK;
+  if (syn0) s = copy_table(h, h ? h->syn0 : nullptr, syn0, row_stride, false);
+  if (s == FW2V_OK && syn1neg) s = copy_table(h, h ? h->syn1neg : nullptr, syn1neg, row_stride, false);
+  return s;
+}
+
+// Shared by fw2v_train_sentences and fw2v_heldout_loss: copy host sentences to
+// temporary device buffers.
+struct DeviceSentences {
+  int32_t* ids = nullptr;
+  int32_t* negs = nullptr;
+  int64_t* starts = nullptr;
+  int32_t* lens = nullptr;
+  float* alphas = nullptr;
+  ~DeviceSentences() {
+    dfree(ids); dfree(negs); dfree(starts); dfree(lens); dfree(alphas);
+  }
+};
+
+static fw2v_status upload_sentences(fw2v_handle* h, DeviceSentences& ds, const int32_t* ids, const int32_t* negs,
+                                    const int64_t* starts, const int32_t* lens, const float* alphas, int64_t n) {
+  const int K = h->cfg.negative;
+  int64_t n_ids = 0;
+  for (int64_t s = 0; s < n; s++) {
+    if (starts[s] < 0 || lens[s] < 0) return fail(h, FW2V_ERR_ARGUMENT, "sentence %lld: negative start/len", (long long)s);
+    n_ids = std::max(n_ids, starts[s] + lens[s]);
+  }
+  CK(h, dalloc(ds.ids, n_ids));
+  CK(h, dalloc(ds.negs, n_ids * std::max(K, 1)));
+  CK(h, dalloc(ds.starts, n));
+  CK(h, dalloc(ds.lens, n));
+  CK(h, dalloc(ds.alphas, n));
+  if (n_ids > 0) {
+    CK(h, cudaMemcpyAsync(ds.ids, ids, n_ids * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+    if (K > 0) CK(h, cudaMemcpyAsync(ds.negs, negs, n_ids * K * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+  }
+  CK(h, cudaMemcpyAsync(ds.starts, starts, n * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(ds.lens, lens, n * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+  if (alphas) CK(h, cudaMemcpyAsync(ds.alphas, alphas, n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+  return FW2V_OK;
+}
+
+fw2v_status fw2v_train_sentences(fw2v_handle* h, const int32_t* ids, const int32_t* negs, const int64_t* starts,
+                                 const int32_t* lens, const float* alphas, int64_t n) {
+  if (!h || n < 0 || (n > 0 && (!ids || !starts || !lens || !alphas || (h->cfg.negative > 0 && !negs))))
+    return fail(h, FW2V_ERR_ARGUMENT, "train_sentences: null input");
+  if (h->V == 0) return fail(h, FW2V_ERR_STATE, "train_sentences before set_vocab");
+  if (n == 0) return FW2V_OK;
+  CK(h, cudaSetDevice(h->cfg.device));
+  DeviceSentences ds;
+  fw2v_status s = upload_sentences(h, ds, ids, negs, starts, lens, alphas, n);
+  if (s != FW2V_OK) return s;
+  TrainParams p = base_train_params(h);
+  p.ids = ds.ids;
+  p.negs = ds.negs;
+  p.source = kSourceExplicit;
+  p.starts = ds.starts;
+  p.lens = ds.lens;
+  p.alphas = ds.alphas;
+  p.n_sentences = n;
+  CK(h, cudaMemsetAsync(h->work_counter, 0, sizeof(unsigned long long), h->stream));
+  CK(h, launch_train(p, h->num_sms, h->stream));
+  return check_flag(h, "train_sentences");
+}
+
+fw2v_status fw2v_heldout_loss(fw2v_handle* h, const int32_t* ids, const int32_t* negs, const int64_t* starts,
+                              const int32_t* lens, int64_t n, double* loss_sum, int64_t* pairs) {
+  if (!h || !loss_sum || !pairs || n < 0) return fail(h, FW2V_ERR_ARGUMENT, "heldout_loss: null output");
+  if (h->V == 0) return fail(h, FW2V_ERR_STATE, "heldout_loss before set_vocab");
+  *loss_sum = 0;
+  *pairs = 0;
+  if (n == 0) return FW2V_OK;
+  CK(h, cudaSetDevice(h->cfg.device));
+  DeviceSentences ds;
+  fw2v_status s = upload_sentences(h, ds, ids, negs, starts, lens, nullptr, n);
+  if (s != FW2V_OK) return s;
+  double* d_loss = nullptr;
+  unsigned long long* d_pairs = nullptr;
+  CK(h, dalloc(d_loss, 1));
+  CK(h, dalloc(d_pairs, 1));
+  CK(h, cudaMemsetAsync(d_loss, 0, sizeof(double), h->stream));
+  CK(h, cudaMemsetAsync(d_pairs, 0, sizeof(unsigned long long), h->stream));
+  TrainParams p = base_train_params(h);
+  p.ids = ds.ids;
+  p.negs = ds.negs;
+  p.starts = ds.starts;
+  p.lens = ds.lens;
+  p.n_sentences = n;
+  CK(h, launch_heldout(p, d_loss, d_pairs, h->stream));
+  unsigned long long np = 0;
+  CK(h, cudaMemcpyAsync(loss_sum, d_loss, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaMemcpyAsync(&np, d_pairs, sizeof(np), cudaMemcpyDeviceToHost, h->stream));
+  s = check_flag(h, "heldout_loss");
+  dfree(d_loss);
+  dfree(d_pairs);
+  *pairs = (int64_t)np;
+  return s;
+}
+
+fw2v_status fw2v_get_unigram(fw2v_handle* h, int64_t first, int64_t n, int32_t* out) {
+  if (!h || !out || first < 0 || n < 0 || first + n > kUnigramTableSize)
+    return fail(h, FW2V_ERR_ARGUMENT, "get_unigram: range");
+  if (!h->unigram) return fail(h, FW2V_ERR_STATE, "get_unigram before set_vocab");
+  CK(h, cudaSetDevice(h->cfg.device));
+  CK(h, cudaMemcpyAsync(out, h->unigram + first, n * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  return FW2V_OK;
+}
+
+}  // extern "C"

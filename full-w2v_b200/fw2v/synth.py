@@ -1,0 +1,198 @@
+"""Seeded synthetic corpora standing in for the reference's text8 / 1-Billion-Word
+/ graph-walk corpora (not available offline): a topic-mixture corpus with
+Zipf-distributed words, and random walks on a stochastic block model.  Both
+come with a planted label per word (topic or block) for precision@10.
+
+`build_stream` turns raw token ids into what the reference's text front end
+would build from the same tokens written one sentence per line: a vocabulary
+sorted by count (ties in first-occurrence order, "</s>" at index 0 with one
+count per line but the last), the min-count cut, and the global token stream
+cut into chunks of `msl` (improved_driver_functions.cpp:136-164, 244-281).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass
+class SynthCorpus:
+    counts: np.ndarray       # uint32, vocab order, index 0 = </s>
+    train_words: int
+    stream: np.ndarray       # int32 vocab ids, trailing 0
+    chunk_off: np.ndarray    # int64
+    label: np.ndarray        # planted topic/block per vocab id (-1 for </s>)
+    raw_of_vocab: np.ndarray  # raw id per vocab id (-1 for </s>)
+
+
+def topic_tokens(n_tokens: int, vocab: int, topics: int, zipf_s: float, *, sentence_len: int = 1000,
+                 dirichlet: float = 0.1, seed: int = 0, chunk: int = 512):
+    """Raw token ids of a topic-mixture corpus, and each raw word's planted topic.
+
+    Every sentence draws topic weights from Dirichlet(dirichlet); every token
+    draws a topic from them and a word from that topic's Zipf(zipf_s) law over
+    its own random permutation of the vocabulary.  A word's planted topic is the
+    topic under which it is most probable (its lowest rank).
+    """
+    rng = np.random.default_rng(seed)
+    perm = np.stack([rng.permutation(vocab) for _ in range(topics)]).astype(np.int32)
+    rank_p = 1.0 / np.arange(1, vocab + 1, dtype=np.float64) ** zipf_s
+    cdf = np.cumsum(rank_p)
+    cdf /= cdf[-1]
+    n_sent = (n_tokens + sentence_len - 1) // sentence_len
+    out = np.empty(n_sent * sentence_len, np.int32)
+    for s0 in range(0, n_sent, chunk):
+        s1 = min(n_sent, s0 + chunk)
+        theta = rng.dirichlet(np.full(topics, dirichlet), size=s1 - s0)
+        ctheta = np.cumsum(theta, axis=1)
+        ctheta[:, -1] = 1.0
+        u = rng.random((s1 - s0, sentence_len))
+        z = np.empty((s1 - s0, sentence_len), np.int32)
+        for i in range(s1 - s0):
+            z[i] = np.searchsorted(ctheta[i], u[i], side="right")
+        np.minimum(z, topics - 1, out=z)
+        r = np.searchsorted(cdf, rng.random((s1 - s0, sentence_len)), side="right")
+        np.minimum(r, vocab - 1, out=r)
+        out[s0 * sentence_len:s1 * sentence_len] = perm[z, r].ravel()
+    ranks = np.empty((topics, vocab), np.int32)
+    ranks[np.arange(topics)[:, None], perm] = np.arange(vocab)[None, :]
+    planted = np.argmin(ranks, axis=0).astype(np.int32)
+    return out[:n_tokens], planted
+
+
+def sbm_walks(nodes: int, blocks: int, degree: float, p_ratio: float, walks_per_node: int,
+              walk_len: int, *, seed: int = 0):
+    """Uniform random walks on a stochastic block model graph.
+
+    Nodes are split into `blocks` equal blocks; edges inside a block are
+    p_ratio times as likely as edges across blocks, with `degree` expected
+    neighbours per node.  Returns (walks as an int32 [n_walks, walk_len] array
+    of node ids, block of each node).
+    """
+    rng = np.random.default_rng(seed)
+    block = (np.arange(nodes) * blocks // nodes).astype(np.int32)
+    bsize = nodes / blocks
+    # expected degree = p_in*(bsize-1) + p_out*(nodes-bsize), p_in = ratio*p_out
+    p_out = degree / (p_ratio * (bsize - 1) + (nodes - bsize))
+    n_in = rng.poisson(p_ratio * p_out * (bsize - 1) * nodes / 2)
+    n_out = rng.poisson(p_out * (nodes - bsize) * nodes / 2)
+    a = rng.integers(0, nodes, n_in)
+    lo = (block[a] * nodes) // blocks
+    hi = ((block[a] + 1) * nodes) // blocks
+    b = lo + (rng.random(n_in) * (hi - lo)).astype(np.int64)
+    c = rng.integers(0, nodes, n_out)
+    dd = rng.integers(0, nodes, n_out)
+    keep = block[c] != block[dd]
+    src = np.concatenate([a, b, c[keep], dd[keep]])
+    dst = np.concatenate([b, a, dd[keep], c[keep]])
+    ok = src != dst
+    src, dst = src[ok], dst[ok]
+    order = np.argsort(src, kind="stable")
+    src, dst = src[order], dst[order].astype(np.int32)
+    offs = np.zeros(nodes + 1, np.int64)
+    np.add.at(offs, src + 1, 1)
+    offs = np.cumsum(offs)
+    deg = np.diff(offs)
+    starts = np.repeat(np.arange(nodes, dtype=np.int32), walks_per_node)
+    walks = np.empty((len(starts), walk_len), np.int32)
+    cur = starts.copy()
+    walks[:, 0] = cur
+    for t in range(1, walk_len):
+        dcur = deg[cur]
+        nxt = cur.copy()
+        has = dcur > 0
+        pick = (rng.random(has.sum()) * dcur[has]).astype(np.int64)
+        nxt[has] = dst[offs[cur[has]] + pick]
+        cur = nxt
+        walks[:, t] = cur
+    return walks, block
+
+
+def build_stream(raw: np.ndarray, sentence_ends: np.ndarray, raw_label: np.ndarray, *,
+                 min_count: int, msl: int, cache_eos: bool = False) -> SynthCorpus:
+    """Vocabulary, stream and chunks for raw ids written one sentence per line.
+
+    sentence_ends: exclusive end offset of each line in `raw`.
+    """
+    n_raw = int(raw.max()) + 1 if len(raw) else 0
+    cnt = np.bincount(raw, minlength=n_raw)
+    first = np.full(n_raw, len(raw), np.int64)
+    np.minimum.at(first, raw, np.arange(len(raw)))
+    seen = np.nonzero(cnt)[0]
+    order = seen[np.lexsort((first[seen], -cnt[seen]))]
+    order = order[cnt[order] >= min_count]
+    n_lines = len(sentence_ends)
+    eos = max(n_lines - 1, 0)  # the final newline is read at EOF and not counted
+    counts = np.concatenate([[eos], cnt[order]]).astype(np.uint32)
+    vocab_of_raw = np.full(n_raw, -1, np.int64)
+    vocab_of_raw[order] = np.arange(1, len(order) + 1)
+    vid = vocab_of_raw[raw]
+    if cache_eos:
+        line = np.zeros(len(raw), np.int64)
+        line[sentence_ends[:-1]] = 1
+        line = np.cumsum(line)
+        keep = vid >= 0
+        toks, pos = [], 0
+        parts = []
+        bounds = np.concatenate([[0], sentence_ends])
+        for i in range(n_lines):
+            seg = vid[bounds[i]:bounds[i + 1]]
+            parts.append(seg[seg >= 0])
+            parts.append(np.zeros(1, np.int64))
+        del toks, pos, keep, line
+        ids = np.concatenate(parts).astype(np.int32)
+        # chunk at EOS or msl (improved_driver_functions.cpp:270)
+        offs, n = [], 0
+        start = True
+        for i, w in enumerate(ids):
+            if start:
+                offs.append(i)
+                start = False
+                n = 0
+            n += 1
+            if w == 0 or n >= msl:
+                start = True
+        chunk_off = np.array(offs, np.int64)
+    else:
+        ids = vid[vid >= 0].astype(np.int32)
+        chunk_off = np.arange(0, len(ids), msl, dtype=np.int64)
+    stream = np.concatenate([ids, np.zeros(1, np.int32)]).astype(np.int32)
+    train_words = int(counts.sum()) + 1
+    label = np.concatenate([[-1], raw_label[order]]).astype(np.int32)
+    raw_of_vocab = np.concatenate([[-1], order]).astype(np.int64)
+    return SynthCorpus(counts, train_words, stream, chunk_off, label, raw_of_vocab)
+
+
+def text_of(raw: np.ndarray, sentence_ends: np.ndarray) -> bytes:
+    """The corpus as a text file: tokens w<raw id>, one sentence per line."""
+    lines, s = [], 0
+    for e in sentence_ends:
+        lines.append(" ".join(f"w{t}" for t in raw[s:e]))
+        s = e
+    return ("\n".join(lines) + "\n").encode()
+
+
+# Workloads of the benchmark configurations (sizes and laws as specified there).
+CONFIGS = {
+    "c1": dict(n_tokens=1_000_000, vocab=10_000, topics=20, zipf_s=1.0, d=100, window=5,
+               negative=5, sample=1e-4, epochs=1, min_count=1),
+    "c2": dict(n_tokens=17_000_000, vocab=71_000, topics=100, zipf_s=1.0, d=128, window=8,
+               negative=5, sample=1e-4, epochs=5, min_count=5),
+    "c3": dict(n_tokens=800_000_000, vocab=555_000, topics=1000, zipf_s=1.05, d=300, window=5,
+               negative=5, sample=1e-4, epochs=1, min_count=5),
+}
+
+
+def make_topic_corpus(name: str, *, n_tokens: int | None = None, seed: int | None = None,
+                      msl: int = 1000) -> tuple[SynthCorpus, dict]:
+    cfg = dict(CONFIGS[name])
+    if n_tokens is not None:
+        cfg["n_tokens"] = n_tokens
+    seed = 1234 + int(name[1:]) if seed is None else seed
+    raw, planted = topic_tokens(cfg["n_tokens"], cfg["vocab"], cfg["topics"], cfg["zipf_s"],
+                                seed=seed)
+    ends = np.arange(1000, len(raw) + 1000, 1000)
+    ends[-1] = len(raw)
+    corpus = build_stream(raw, ends, planted, min_count=cfg["min_count"], msl=msl)
+    return corpus, cfg

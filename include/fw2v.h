@@ -1,0 +1,197 @@
+/*
+ * fw2v.h — C ABI of libfw2v.so, the B200 SGNS (skip-gram negative sampling)
+ * trainer that replaces the FULL-W2V training path.
+ *
+ * Plain C types only; every call returns an fw2v_status and never exits the
+ * process.  A handle owns all device memory it allocates and must be used from
+ * one host thread at a time.  Streams and graphs are internal.
+ *
+ * What each entry point replaces in the reference (tlranda/FULL-W2V, paths
+ * relative to its root):
+ *
+ *   fw2v_create / fw2v_destroy     global configuration + teardown,
+ *                                  src/FULL-W2V/FULL-W2V-driver.cu:42-73, 453-470
+ *   fw2v_set_vocab                 InitNet: syn0 LCG init, syn1neg zero, unigram
+ *                                  table, subsampling table,
+ *                                  src/FULL-W2V/improved_driver_functions.cpp:1-83
+ *   fw2v_load_corpus               the global token stream and its sentence
+ *                                  table (createGlobalStream / readCorpusCache),
+ *                                  improved_driver_functions.cpp:244-281, 320-401
+ *   fw2v_sample_epoch              the host batch builder of Train_SGNS (LCG
+ *                                  subsampling + negatives + alpha schedule),
+ *                                  FULL-W2V-driver.cu:166-302, moved on-device
+ *   fw2v_train_sampled             the kernel launches of Train_SGNS,
+ *                                  FULL-W2V-driver.cu:284-299, 305-319
+ *   fw2v_train_epoch / fw2v_train  one / all epochs of Train_SGNS,
+ *                                  FULL-W2V-driver.cu:80-354, 438-446
+ *   fw2v_kernel_batch              the `cuda_kernel` function-pointer seam
+ *                                  (FULL-W2V-kernels.cu:11-12, bound at :24,
+ *                                  called at FULL-W2V-driver.cu:293, 317) with
+ *                                  the same arguments: device sentence, negative,
+ *                                  length and alpha arrays laid out per block
+ *   fw2v_get_syn0 / fw2v_get_syn1neg
+ *                                  the device-to-host copy of saveModel,
+ *                                  improved_driver_functions.cpp:225-228
+ *   fw2v_words_trained             word_count_actual, the numerator of
+ *                                  "Overall Words Per Second", FULL-W2V-driver.cu:450-451
+ */
+#ifndef FW2V_H
+#define FW2V_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum fw2v_status {
+  FW2V_OK = 0,
+  FW2V_ERR_ARGUMENT = 1,     /* invalid argument or unsupported size */
+  FW2V_ERR_CUDA = 2,         /* a CUDA runtime call failed; see fw2v_last_error */
+  FW2V_ERR_NOMEM = 3,        /* device or pinned host allocation failed */
+  FW2V_ERR_STATE = 4,        /* call out of order (e.g. train before set_vocab) */
+  FW2V_ERR_BOUNDS = 5,       /* a token or negative id outside [0, V) was found */
+  FW2V_ERR_NO_DEVICE = 6     /* no CUDA device or the library was built for another arch */
+} fw2v_status;
+
+typedef enum fw2v_sigmoid {
+  FW2V_SIGMOID_TABLE = 0,    /* the reference's 1000-entry table (expTable.h) */
+  FW2V_SIGMOID_EXACT = 1     /* 1/(1+expf(-x)) */
+} fw2v_sigmoid;
+
+typedef enum fw2v_precision {
+  FW2V_FP32 = 0,             /* FP32 tables, FP32 math */
+  FW2V_BF16 = 1              /* BF16 tables, FP32 math, stochastic-rounded write-back */
+} fw2v_precision;
+
+typedef struct fw2v_config {
+  int32_t layer_size;        /* -size  d, 1..1024 */
+  int32_t window;            /* -window W, 1..15 */
+  int32_t negative;          /* -negative K, 0..31 */
+  int32_t epochs;            /* -iter E */
+  int32_t threads;           /* -threads T: sampling streams, each seeded with its id */
+  int32_t msl;               /* -msl: maximum kept words per sentence */
+  float alpha;               /* -alpha: starting learning rate */
+  float sample;              /* -sample: subsampling threshold (0 disables) */
+  int32_t sigmoid;           /* fw2v_sigmoid */
+  int32_t precision;         /* fw2v_precision */
+  int32_t deterministic;     /* 1: sentences trained one at a time in stream order */
+  int32_t device;            /* CUDA device ordinal */
+} fw2v_config;
+
+typedef struct fw2v_handle fw2v_handle;
+
+typedef struct fw2v_epoch_stats {
+  uint64_t words_read;       /* tokens read this epoch, subsampled-away and EOS included */
+  uint64_t words_kept;       /* tokens that survived subsampling in trained sentences */
+  uint64_t sentences;        /* batch entries recorded (zero-length ones included) */
+  float sampler_ms;          /* device time of the sampling kernel */
+  float train_ms;            /* device time of the training kernel */
+} fw2v_epoch_stats;
+
+/* Fill *cfg with the reference defaults (FULL-W2V-driver.cu:49-55,
+ * improved_driver_functions.cpp:475-501). */
+void fw2v_config_default(fw2v_config* cfg);
+
+fw2v_status fw2v_create(const fw2v_config* cfg, fw2v_handle** out);
+void fw2v_destroy(fw2v_handle* h);
+
+/* Vocabulary in reference order (index 0 = "</s>", then descending count).
+ * train_words is the reference's train_words (sum of kept counts, +1 when
+ * learned from a text file).  Allocates and initialises the embedding tables. */
+fw2v_status fw2v_set_vocab(fw2v_handle* h, const uint32_t* counts, int64_t vocab_size,
+                           uint64_t train_words);
+
+/* Token stream (host memory; ids in [0, V), the trailing 0 included) and the
+ * start offset of each stored sentence chunk.  Requires threads <= n_chunks. */
+fw2v_status fw2v_load_corpus(fw2v_handle* h, const int32_t* stream, int64_t stream_len,
+                             const int64_t* chunk_off, int64_t n_chunks);
+
+/* Run the on-device batch builder for the next epoch only. */
+fw2v_status fw2v_sample_epoch(fw2v_handle* h);
+/* Sizes of the last sampled epoch: entries and kept ids summed over streams. */
+fw2v_status fw2v_epoch_sample_sizes(fw2v_handle* h, int64_t* n_entries, int64_t* n_kept);
+/* Copy the last sampled epoch to host memory, streams in order.  Per stream s:
+ * entries_per_stream[s] entries (lens, alphas) and kept_per_stream[s] kept ids
+ * (ids) with `negative` negatives each (negs); words_per_stream[s] tokens read.
+ * Any output pointer may be NULL. */
+fw2v_status fw2v_epoch_samples(fw2v_handle* h, int32_t* lens, float* alphas, int32_t* ids,
+                               int32_t* negs, int64_t* entries_per_stream,
+                               int64_t* kept_per_stream, uint64_t* words_per_stream);
+/* Train the sentences of the last sampled epoch. */
+fw2v_status fw2v_train_sampled(fw2v_handle* h, fw2v_epoch_stats* stats);
+
+/* Sample + train one epoch; stats may be NULL. */
+fw2v_status fw2v_train_epoch(fw2v_handle* h, fw2v_epoch_stats* stats);
+/* Run the remaining epochs of the configured E. */
+fw2v_status fw2v_train(fw2v_handle* h, uint64_t* words_read);
+
+/* Total tokens read over all epochs trained so far. */
+fw2v_status fw2v_words_trained(fw2v_handle* h, uint64_t* words);
+
+/* Copy tables to/from host memory, rows of layer_size floats spaced by
+ * row_stride floats (row_stride >= layer_size). */
+fw2v_status fw2v_get_syn0(fw2v_handle* h, float* out, int64_t row_stride);
+fw2v_status fw2v_get_syn1neg(fw2v_handle* h, float* out, int64_t row_stride);
+fw2v_status fw2v_set_tables(fw2v_handle* h, const float* syn0, const float* syn1neg,
+                            int64_t row_stride);
+
+/* Train explicit sentences from host memory (deterministic order when the
+ * handle is deterministic): sentence s has lens[s] ids starting at
+ * ids[starts[s]] and negatives at negs[starts[s] * K]. */
+fw2v_status fw2v_train_sentences(fw2v_handle* h, const int32_t* ids, const int32_t* negs,
+                                 const int64_t* starts, const int32_t* lens, const float* alphas,
+                                 int64_t n_sentences);
+
+/* Held-out SGNS loss summed in FP64 on the device over every (context, centre)
+ * pair of the given sentences: -log s(<v_c,o_w>) - sum_k log s(-<v_c,o_nk>). */
+fw2v_status fw2v_heldout_loss(fw2v_handle* h, const int32_t* ids, const int32_t* negs,
+                              const int64_t* starts, const int32_t* lens, int64_t n_sentences,
+                              double* loss_sum, int64_t* pairs);
+
+/* The reference kernel seam: FP32 tables with `pitch` floats per row, block b
+ * trains sen[b*msl .. +len[b]] with negatives neg[b*msl*K ...] at alpha[b].
+ * All pointers are device pointers; `stream` is a cudaStream_t (NULL: default).
+ * The launch is asynchronous; errors found by the kernel (ids outside
+ * [0, vocab_size)) are reported by the next call on the same handle-less seam
+ * through fw2v_kernel_batch_error. */
+fw2v_status fw2v_kernel_batch(float* syn0, float* syn1neg, const int32_t* sen, const int32_t* neg,
+                              const int32_t* len, const float* alpha, int32_t n_blocks,
+                              int32_t layer_size, int32_t window, int32_t negative, int32_t msl,
+                              uint32_t pitch, int64_t vocab_size, void* stream);
+/* Returns FW2V_ERR_BOUNDS (and clears it) if an earlier fw2v_kernel_batch launch
+ * on this device skipped a block with an out-of-range id; synchronises `stream`. */
+fw2v_status fw2v_kernel_batch_error(void* stream);
+
+/* Host-only helpers (no device needed).
+ * fw2v_lane_layout: the device row layout for a layer size: rows hold `pitch`
+ * values (FP32: layer_size rounded up to 8) and lane l of a warp owns elements
+ * ((i*32+l)*vec + j), i < nv, j < vec; dot products sum each lane's elements in
+ * that order and combine lanes with an xor tree (16, 8, 4, 2, 1).
+ * fw2v_exp_table: the 1000-entry sigmoid table of generate_expTable_h.cpp:46-55.
+ * fw2v_unigram_firsts: first index of words 1..V-1 in the reference unigram
+ * table of `table_size` entries (improved_driver_functions.cpp:44-58); words
+ * never reached get table_size.  Returns 0, or -1 if V < 2. */
+void fw2v_lane_layout(int32_t layer_size, int32_t precision, int32_t* vec, int32_t* nv,
+                      int64_t* pitch);
+void fw2v_exp_table(float* table);
+int fw2v_unigram_firsts(const uint32_t* counts, int64_t vocab_size, int64_t table_size,
+                        int64_t* firsts);
+/* Copy n entries of the device unigram table starting at index `first`. */
+fw2v_status fw2v_get_unigram(fw2v_handle* h, int64_t first, int64_t n, int32_t* out);
+
+/* The handle's CUDA stream (a cudaStream_t), on which every kernel of the
+ * handle runs; lets a caller time or order its own work against the epochs. */
+void* fw2v_stream(fw2v_handle* h);
+
+const char* fw2v_status_string(fw2v_status s);
+/* Detail of the last error on this handle (empty string if none). */
+const char* fw2v_last_error(fw2v_handle* h);
+/* Library build information, e.g. "fw2v sm_100a". */
+const char* fw2v_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

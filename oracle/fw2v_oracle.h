@@ -126,6 +126,12 @@ double orc_heldout_loss(const float* syn0, const float* syn1neg, int64_t pitch, 
                         int negative, int64_t n_sent, const int64_t* starts, const int32_t* lens,
                         const int32_t* ids, const int32_t* negs, int64_t* pairs);
 
+/* Timed CPU baseline (fw2v_cpu_sgns.c): every stream sampled and trained by
+ * n_threads host threads on shared tables (Hogwild), FP32. */
+int orc_cpu_sgns(const orc_sampler_cfg* scfg, const orc_train_cfg* tcfg, float* syn0, float* syn1neg,
+                 int n_threads, int64_t max_entries_per_stream, uint64_t* words_read,
+                 uint64_t* words_kept);
+
 #ifdef __cplusplus
 }
 #endif

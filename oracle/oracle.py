@@ -79,6 +79,9 @@ def _declare(L):
         f = getattr(L, name)
         f.restype = C.c_int
         f.argtypes = [C.POINTER(TrainCfg), P, P, C.c_int64, C.c_int64, P, P, P, P, P]
+    L.orc_cpu_sgns.restype = C.c_int
+    L.orc_cpu_sgns.argtypes = [C.POINTER(SamplerCfg), C.POINTER(TrainCfg), P, P, C.c_int,
+                               C.c_int64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.orc_heldout_loss.restype = C.c_double
     L.orc_heldout_loss.argtypes = [P, P, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int64,
                                    P, P, P, P, C.POINTER(C.c_int64)]
@@ -188,6 +191,34 @@ def sample_streams(corpus: Corpus, *, threads: int, msl: int, negative: int, epo
                                          negs[: k * negative].copy(), int(wr.value)))
         out.append(per_epoch)
     return out
+
+
+def cpu_sgns(corpus: Corpus, syn0, syn1neg, *, threads: int, msl: int, negative: int,
+             epochs: int, alpha0: float, sample: float, d: int, window: int, n_threads: int,
+             max_entries_per_stream: int = 0, sigmoid: str = "table"):
+    """Timed CPU baseline: sample + train every stream on n_threads host threads.
+
+    Returns (words_read, words_kept); tables are updated in place (Hogwild)."""
+    L = lib()
+    stream = np.ascontiguousarray(corpus.stream, np.int32)
+    chunk_off = np.ascontiguousarray(corpus.chunk_off, np.int64)
+    counts = np.ascontiguousarray(corpus.counts, np.uint32)
+    p_keep = subsample_table(counts, sample, corpus.train_words) if sample > 0 else \
+        np.zeros(len(counts), np.float32)
+    rs, rw = unigram_runs(counts)
+    scfg = SamplerCfg(_p(stream).value, len(stream), _p(chunk_off).value, len(chunk_off),
+                      _p(p_keep).value, sample, _p(rs).value, _p(rw).value, len(rw),
+                      UNIGRAM_TABLE_SIZE, threads, msl, negative, epochs, alpha0,
+                      corpus.train_words)
+    table = exp_table()
+    tcfg = _train_cfg(d, syn0.shape[1], window, negative, 0 if sigmoid == "table" else 1, 4, 1,
+                      table)
+    wr, wk = C.c_uint64(), C.c_uint64()
+    rc = L.orc_cpu_sgns(C.byref(scfg), C.byref(tcfg), _p(syn0), _p(syn1neg), n_threads,
+                        max_entries_per_stream, C.byref(wr), C.byref(wk))
+    if rc != 0:
+        raise RuntimeError(f"orc_cpu_sgns failed: {rc}")
+    return int(wr.value), int(wk.value)
 
 
 def _train_cfg(d, pitch, window, negative, sigmoid, vec, nv, table):

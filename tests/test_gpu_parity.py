@@ -1,0 +1,298 @@
+"""GPU parity of libfw2v against the oracle and the reference's golden dumps.
+
+Integer work (sampling, negatives, unigram table, syn0 init, word counts) must
+match bit for bit.  The training update is checked in deterministic mode:
+  * table sigmoid against the oracle's FP32 mode, which reproduces the kernel's
+    operation order: bit for bit;
+  * exact sigmoid against the oracle's FP64 mode: max |gpu - fp64| <= 1e-5 *
+    max|fp64| per table (the tolerance of the north-star spec, "within 1e-5
+    relative").
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+import fw2v
+from golden_cases import CASES, load
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL_FP64 = 1e-5
+
+
+def corpus_of(g):
+    c = g["cfg"]
+    return O.corpus_from_text(g["text"], min_count=c["min_count"], msl=c["msl"],
+                              cache_eos=c["cache_eos"])
+
+
+def trainer_for(corpus, c, **kw):
+    cfg = fw2v.default_config(layer_size=kw.pop("layer_size", c["size"]), window=c["window"],
+                              negative=c["negative"], epochs=c["iter"], threads=c["threads"],
+                              msl=c["msl"], alpha=c["alpha"], sample=c["sample"], **kw)
+    t = fw2v.Trainer(cfg)
+    t.set_vocab(corpus.counts, corpus.train_words)
+    t.load_corpus(corpus.stream, corpus.chunk_off)
+    return t
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_sampler_matches_reference_dumps(name):
+    g = load(name)
+    c = g["cfg"]
+    corpus = corpus_of(g)
+    ref = g["threads_out"]
+    with trainer_for(corpus, c) as t:
+        per_stream = [[] for _ in range(c["threads"])]
+        words = 0
+        for _ in range(c["iter"]):
+            t.sample_epoch()
+            for s, rec in enumerate(t.epoch_samples()):
+                per_stream[s].append(rec)
+                words += rec[4]
+            t.train_sampled()
+        assert words == int(g["overall_words"])
+        assert t.words_trained() == int(g["overall_words"])
+    unmatched = list(range(len(ref)))
+    for s, recs in enumerate(per_stream):
+        lens = np.concatenate([r[0] for r in recs])
+        ids = np.concatenate([r[2] for r in recs])
+        hit = [k for k in unmatched if np.array_equal(ref[k]["lens"], lens)
+               and np.array_equal(ref[k]["ids"], ids)]
+        assert hit, f"stream {s} differs from every reference thread"
+        unmatched.remove(hit[0])
+        np.testing.assert_array_equal(np.concatenate([r[3] for r in recs]), ref[hit[0]]["negs"])
+        if c["threads"] == 1:
+            np.testing.assert_array_equal(np.concatenate([r[1] for r in recs]),
+                                          ref[hit[0]]["alphas"])
+
+
+@pytest.mark.parametrize("name", ["zipf_t1", "eos_t1"])
+def test_syn0_init_and_unigram_table(name):
+    g = load(name)
+    c = g["cfg"]
+    corpus = corpus_of(g)
+    with trainer_for(corpus, c) as t:
+        s0 = t.syn0()
+        assert hashlib.sha256(s0.tobytes()).hexdigest() == str(g["syn0_init_sha256"])
+        assert not t.syn1neg().any()
+        starts, words = O.unigram_runs(corpus.counts)
+        # every run boundary and a random sample of the 1e8 entries
+        probe = np.unique(np.concatenate([starts[:-1], np.maximum(starts[1:] - 1, 0),
+                                          np.random.default_rng(0).integers(0, O.UNIGRAM_TABLE_SIZE,
+                                                                            20000)]))
+        got = np.array([t.unigram(int(i), 1)[0] for i in probe[:2000]])
+        want = np.array([words[np.searchsorted(starts, i, side="right") - 1] for i in probe[:2000]])
+        np.testing.assert_array_equal(got, want)
+        block = t.unigram(0, 1_000_000)
+        want_block = words[np.searchsorted(starts, np.arange(1_000_000), side="right") - 1]
+        np.testing.assert_array_equal(block, want_block)
+
+
+def _oracle_epoch(corpus, c):
+    out = O.sample_streams(corpus, threads=c["threads"], msl=c["msl"], negative=c["negative"],
+                           epochs=c["iter"], alpha0=c["alpha"], sample=c["sample"])
+    return out
+
+
+def _flatten_epoch(out, e):
+    lens = np.concatenate([out[s][e].lens for s in range(len(out))])
+    alphas = np.concatenate([out[s][e].alphas for s in range(len(out))])
+    ids = np.concatenate([out[s][e].ids for s in range(len(out))])
+    negs = np.concatenate([out[s][e].negs for s in range(len(out))])
+    return lens, alphas, ids, negs
+
+
+@pytest.mark.parametrize("name,d", [("zipf_t1", 8), ("zipf_t1", 100), ("eos_t1", 128),
+                                    ("zipf_t3", 300), ("k0_t1", 64), ("messy_t1", 40),
+                                    ("nosample_t2", 200)])
+def test_deterministic_training_bit_exact_fp32_table_sigmoid(name, d):
+    g = load(name)
+    c = dict(g["cfg"])
+    c["iter"] = 1
+    corpus = corpus_of(g)
+    vec, nv, pitch = fw2v.lane_layout(d)
+    with trainer_for(corpus, c, layer_size=d, deterministic=1) as t:
+        syn0 = np.zeros((len(corpus.counts), d), np.float32)
+        syn0[:] = t.syn0()
+        syn1 = np.zeros_like(syn0)
+        t.train_epoch()
+        got0, got1 = t.syn0(), t.syn1neg()
+    out = _oracle_epoch(corpus, c)
+    lens, alphas, ids, negs = _flatten_epoch(out, 0)
+    O.train(syn0, syn1, lens, alphas, ids, negs, d=d, window=c["window"], negative=c["negative"],
+            sigmoid="table", precision=32, vec=vec, nv=nv)
+    assert np.abs(got0 - syn0).max() == 0 and np.abs(got1 - syn1).max() == 0, \
+        (np.abs(got0 - syn0).max(), np.abs(got1 - syn1).max())
+    assert np.abs(got1).max() > 0
+
+
+@pytest.mark.parametrize("name,d", [("zipf_t1", 100), ("eos_t1", 128), ("zipf_t3", 300)])
+def test_deterministic_training_exact_sigmoid_within_1e5_of_fp64(name, d):
+    g = load(name)
+    c = dict(g["cfg"])
+    c["iter"] = 1
+    corpus = corpus_of(g)
+    with trainer_for(corpus, c, layer_size=d, deterministic=1, sigmoid=fw2v.SIGMOID_EXACT) as t:
+        syn0 = t.syn0().astype(np.float64)
+        syn1 = np.zeros_like(syn0)
+        t.train_epoch()
+        got0, got1 = t.syn0(), t.syn1neg()
+    lens, alphas, ids, negs = _flatten_epoch(_oracle_epoch(corpus, c), 0)
+    O.train(syn0, syn1, lens, alphas, ids, negs, d=d, window=c["window"], negative=c["negative"],
+            sigmoid="exact", precision=64)
+    for got, ref in ((got0, syn0), (got1, syn1)):
+        err = np.abs(got - ref).max() / np.abs(ref).max()
+        assert err <= REL_TOL_FP64, err
+
+
+def test_per_step_update_within_1e5_of_fp64():
+    """One sentence at a time from the GPU's own state: each step's update is
+    within 1e-5 relative of FP64 arithmetic applied to the same input state."""
+    g = load("zipf_t1")
+    c = dict(g["cfg"])
+    c["iter"] = 1
+    corpus = corpus_of(g)
+    d = 128
+    lens, alphas, ids, negs = _flatten_epoch(_oracle_epoch(corpus, c), 0)
+    starts = np.concatenate([[0], np.cumsum(lens[:-1])]).astype(np.int64)
+    K = c["negative"]
+    with trainer_for(corpus, c, layer_size=d, deterministic=1, sigmoid=fw2v.SIGMOID_EXACT) as t:
+        rng = np.random.default_rng(3)
+        t.set_tables(t.syn0(), (rng.standard_normal((len(corpus.counts), d)) * 0.05).astype(np.float32))
+        worst = 0.0
+        for s in [i for i in range(len(lens)) if lens[i] > 0][:12]:
+            a0, a1 = t.syn0(), t.syn1neg()
+            sl = slice(starts[s], starts[s] + lens[s])
+            sid, sneg = ids[sl], negs[starts[s] * K:(starts[s] + lens[s]) * K]
+            t.train_sentences([lens[s]], [alphas[s]], sid, sneg)
+            b0, b1 = t.syn0(), t.syn1neg()
+            r0, r1 = a0.astype(np.float64), a1.astype(np.float64)
+            O.train(r0, r1, [lens[s]], [alphas[s]], sid, sneg, d=d, window=c["window"],
+                    negative=K, sigmoid="exact", precision=64)
+            # compare the change each table received
+            for got, ref, before in ((b0, r0, a0), (b1, r1, a1)):
+                dg = got.astype(np.float64) - before
+                dr = ref - before
+                if np.abs(dr).max() > 0:
+                    worst = max(worst, np.abs(dg - dr).max() / np.abs(dr).max())
+        assert worst <= REL_TOL_FP64, worst
+
+
+def test_duplicate_targets_and_short_sentences_bit_exact():
+    """Centres whose targets repeat (serial path), sentences shorter than the
+    window, and K=5 with repeated negatives."""
+    V, d, W, K = 50, 128, 4, 5
+    rng = np.random.default_rng(7)
+    lens = np.array([1, 2, 3, 9, 10, 40, 5, 17], np.int32)
+    n = int(lens.sum())
+    ids = rng.integers(1, 8, n).astype(np.int32)           # few words: many repeats
+    negs = rng.integers(1, 6, n * K).astype(np.int32)       # repeated negatives
+    alphas = np.full(len(lens), 0.05, np.float32)
+    counts = np.arange(V, 0, -1).astype(np.uint32)
+    vec, nv, _ = fw2v.lane_layout(d)
+    cfg = fw2v.default_config(layer_size=d, window=W, negative=K, threads=1, deterministic=1)
+    with fw2v.Trainer(cfg) as t:
+        t.set_vocab(counts, int(counts.sum()))
+        syn1 = (rng.standard_normal((V, d)) * 0.1).astype(np.float32)
+        t.set_tables(None, syn1)
+        syn0 = t.syn0()
+        t.train_sentences(lens, alphas, ids, negs)
+        got0, got1 = t.syn0(), t.syn1neg()
+    O.train(syn0, syn1, lens, alphas, ids, negs, d=d, window=W, negative=K, sigmoid="table",
+            precision=32, vec=vec, nv=nv)
+    np.testing.assert_array_equal(got0, syn0)
+    np.testing.assert_array_equal(got1, syn1)
+
+
+def test_hogwild_epoch_runs_and_learns():
+    g = load("zipf_t1")
+    c = dict(g["cfg"])
+    corpus = corpus_of(g)
+    with trainer_for(corpus, c, layer_size=64) as t:
+        lens, alphas, ids, negs = _flatten_epoch(_oracle_epoch(corpus, dict(c, iter=1)), 0)
+        before, _ = t.heldout_loss(lens, ids, negs)
+        words = t.train()
+        after, pairs = t.heldout_loss(lens, ids, negs)
+        s0 = t.syn0()
+    assert words == int(g["overall_words"])
+    assert np.isfinite(s0).all()
+    assert after < before
+
+
+def test_heldout_loss_matches_oracle():
+    g = load("eos_t1")
+    c = dict(g["cfg"])
+    corpus = corpus_of(g)
+    d = 96
+    lens, alphas, ids, negs = _flatten_epoch(_oracle_epoch(corpus, dict(c, iter=1)), 0)
+    with trainer_for(corpus, c, layer_size=d) as t:
+        rng = np.random.default_rng(1)
+        t.set_tables(None, (rng.standard_normal((len(corpus.counts), d)) * 0.1).astype(np.float32))
+        loss, pairs = t.heldout_loss(lens, ids, negs)
+        s0, s1 = t.syn0(), t.syn1neg()
+    ref, ref_pairs = O.heldout_loss(s0, s1, lens, ids, negs, d=d, window=c["window"],
+                                    negative=c["negative"])
+    assert pairs == ref_pairs
+    assert abs(loss - ref) <= 1e-9 * abs(ref)
+
+
+def test_kernel_seam_matches_oracle():
+    """fw2v_kernel_batch with the reference's batch layout (device buffers), one
+    block per launch so the result is deterministic."""
+    import torch
+    V, d, W, K, msl = 64, 128, 3, 4, 20
+    rng = np.random.default_rng(11)
+    nb = 6
+    lens = rng.integers(0, msl + 1, nb).astype(np.int32)
+    sen = rng.integers(1, V, (nb, msl)).astype(np.int32)
+    neg = rng.integers(1, V, (nb, msl, K)).astype(np.int32)
+    alphas = np.full(nb, 0.03, np.float32)
+    pitch = 128
+    syn0 = (rng.standard_normal((V, pitch)) * 0.05).astype(np.float32)
+    syn1 = (rng.standard_normal((V, pitch)) * 0.05).astype(np.float32)
+    dev = torch.device("cuda:0")
+    t0, t1 = torch.from_numpy(syn0).to(dev), torch.from_numpy(syn1).to(dev)
+    ts, tn = torch.from_numpy(sen).to(dev), torch.from_numpy(neg).to(dev)
+    tl, ta = torch.from_numpy(lens).to(dev), torch.from_numpy(alphas).to(dev)
+    L = fw2v.lib()
+    for b in range(nb):
+        st = L.fw2v_kernel_batch(t0.data_ptr(), t1.data_ptr(), ts[b].data_ptr(), tn[b].data_ptr(),
+                                 tl[b:].data_ptr(), ta[b:].data_ptr(), 1, d, W, K, msl, pitch, V,
+                                 None)
+        assert st == 0
+    assert L.fw2v_kernel_batch_error(None) == 0
+    vec, nv, _ = fw2v.lane_layout(d)
+    flat_ids = np.concatenate([sen[b, :lens[b]] for b in range(nb)])
+    flat_negs = np.concatenate([neg[b, :lens[b]].ravel() for b in range(nb)])
+    O.train(syn0, syn1, lens, alphas, flat_ids, flat_negs, d=d, window=W, negative=K,
+            sigmoid="table", precision=32, vec=vec, nv=nv)
+    np.testing.assert_array_equal(t0.cpu().numpy(), syn0)
+    np.testing.assert_array_equal(t1.cpu().numpy(), syn1)
+    # an out-of-range id is skipped and reported, and the seam stays usable
+    bad = ts[0].clone()
+    bad[0] = V + 5
+    tl[0] = 3
+    assert L.fw2v_kernel_batch(t0.data_ptr(), t1.data_ptr(), bad.data_ptr(), tn[0].data_ptr(),
+                               tl.data_ptr(), ta.data_ptr(), 1, d, W, K, msl, pitch, V, None) == 0
+    assert L.fw2v_kernel_batch_error(None) == 5
+    assert L.fw2v_kernel_batch_error(None) == 0
+
+
+def test_out_of_range_ids_are_rejected_and_handle_survives():
+    V, d = 20, 64
+    counts = np.arange(V, 0, -1).astype(np.uint32)
+    with fw2v.Trainer(fw2v.default_config(layer_size=d, window=2, negative=2, threads=1)) as t:
+        t.set_vocab(counts, int(counts.sum()))
+        with pytest.raises(fw2v.Fw2vError) as e:
+            t.train_sentences([3], [0.02], np.array([1, 2, V], np.int32),
+                              np.ones(6, np.int32))
+        assert e.value.status == 5
+        bad_stream = np.array([1, 2, V + 1, 0], np.int32)
+        with pytest.raises(fw2v.Fw2vError) as e:
+            t.load_corpus(bad_stream, np.array([0], np.int64))
+        assert e.value.status == 5
+        t.train_sentences([3], [0.02], np.array([1, 2, 3], np.int32), np.ones(6, np.int32))
+        assert np.isfinite(t.syn0()).all()
