@@ -16,11 +16,11 @@ extern "C" void fw2v_exp_table(float* t);
 extern "C" int fw2v_unigram_firsts(const uint32_t* counts, int64_t V, int64_t size, int64_t* firsts);
 
 namespace fw2v {
-cudaError_t launch_sampler(const SamplerParams& p, int64_t* entry_prefix, cudaStream_t st);
+cudaError_t launch_sampler(const SamplerParams& p, int64_t max_region, int64_t* entry_prefix, cudaStream_t st);
 cudaError_t launch_train(const TrainParams& p, int num_sms, cudaStream_t st);
 cudaError_t launch_heldout(const TrainParams& p, double* loss, unsigned long long* pairs, cudaStream_t st);
 cudaError_t launch_init_tables(float* syn0, int64_t V, int d, int64_t pitch, const uint32_t* d_counts,
-                               float sample, uint64_t train_words, float* p_keep, const int64_t* d_firsts,
+                               float sample, uint64_t train_words, int32_t* keep_thr, const int64_t* d_firsts,
                                int n_firsts, int32_t* unigram, int64_t table_size, cudaStream_t st);
 size_t train_smem_bytes(int window, int64_t pitch, int warps);
 cudaError_t launch_validate_ids(const int32_t* ids, int64_t n, int64_t vocab, int* flag, cudaStream_t st);
@@ -40,14 +40,17 @@ struct fw2v_handle {
   int64_t pitch = 0;
   float* syn0 = nullptr;
   float* syn1neg = nullptr;
-  float* p_keep = nullptr;
+  int32_t* keep_thr = nullptr;
   int32_t* unigram = nullptr;
+  uint64_t* jump_a = nullptr;
+  uint64_t* jump_c = nullptr;
   float* exp_table = nullptr;
 
   int32_t* stream_ids = nullptr;
   int64_t stream_len = 0;
   int64_t* chunk_off = nullptr;
   int64_t n_chunks = 0;
+  int64_t max_region = 0;
 
   uint64_t* lcg = nullptr;
   uint64_t* wca = nullptr;
@@ -56,6 +59,7 @@ struct fw2v_handle {
   int32_t* ent_len = nullptr;
   float* ent_alpha = nullptr;
   int32_t* kept_ids = nullptr;
+  uint64_t* kept_state = nullptr;
   int32_t* kept_negs = nullptr;
   int64_t* n_entries = nullptr;
   int64_t* n_kept = nullptr;
@@ -219,6 +223,19 @@ fw2v_status fw2v_create(const fw2v_config* cfg, fw2v_handle** out) {
   if (dalloc(h->error_flag, 1) != cudaSuccess || dalloc(h->work_counter, 1) != cudaSuccess ||
       dalloc(h->exp_table, kExpTableSize) != cudaSuccess)
     return cleanup(FW2V_ERR_NOMEM);
+  // LCG jump-ahead table for up to 32 tokens of 1+K steps each.
+  const int n_jump = 32 * (1 + c.negative) + 1;
+  std::vector<uint64_t> ja(n_jump), jc(n_jump);
+  for (int m = 0; m < n_jump; m++) {
+    const Affine j = lcg_jump((uint64_t)m);
+    ja[m] = j.a;
+    jc[m] = j.c;
+  }
+  if (dalloc(h->jump_a, n_jump) != cudaSuccess || dalloc(h->jump_c, n_jump) != cudaSuccess)
+    return cleanup(FW2V_ERR_NOMEM);
+  if (cudaMemcpy(h->jump_a, ja.data(), n_jump * sizeof(uint64_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(h->jump_c, jc.data(), n_jump * sizeof(uint64_t), cudaMemcpyHostToDevice) != cudaSuccess)
+    return cleanup(FW2V_ERR_CUDA);
   float table[kExpTableSize];
   fw2v_exp_table(table);
   if (cudaMemcpy(h->exp_table, table, sizeof(table), cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -232,7 +249,8 @@ void fw2v_destroy(fw2v_handle* h) {
   if (!h) return;
   cudaSetDevice(h->cfg.device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  dfree(h->syn0); dfree(h->syn1neg); dfree(h->p_keep); dfree(h->unigram); dfree(h->exp_table);
+  dfree(h->syn0); dfree(h->syn1neg); dfree(h->keep_thr); dfree(h->unigram); dfree(h->exp_table);
+  dfree(h->jump_a); dfree(h->jump_c); dfree(h->kept_state);
   dfree(h->stream_ids); dfree(h->chunk_off);
   dfree(h->lcg); dfree(h->wca); dfree(h->alpha);
   dfree(h->ent_start); dfree(h->ent_len); dfree(h->ent_alpha);
@@ -254,7 +272,7 @@ fw2v_status fw2v_set_vocab(fw2v_handle* h, const uint32_t* counts, int64_t V, ui
   h->train_words = train_words;
   CK(h, dalloc(h->syn0, (size_t)V * P));
   CK(h, dalloc(h->syn1neg, (size_t)V * P));
-  CK(h, dalloc(h->p_keep, V));
+  CK(h, dalloc(h->keep_thr, V));
   CK(h, dalloc(h->unigram, kUnigramTableSize));
   CK(h, cudaMemsetAsync(h->syn0, 0, (size_t)V * P * sizeof(float), h->stream));
   CK(h, cudaMemsetAsync(h->syn1neg, 0, (size_t)V * P * sizeof(float), h->stream));
@@ -266,7 +284,7 @@ fw2v_status fw2v_set_vocab(fw2v_handle* h, const uint32_t* counts, int64_t V, ui
   CK(h, dalloc(d_firsts, V - 1));
   CK(h, cudaMemcpyAsync(d_counts, counts, V * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaMemcpyAsync(d_firsts, firsts.data(), (V - 1) * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
-  CK(h, launch_init_tables(h->syn0, V, d, P, d_counts, h->cfg.sample, train_words, h->p_keep, d_firsts,
+  CK(h, launch_init_tables(h->syn0, V, d, P, d_counts, h->cfg.sample, train_words, h->keep_thr, d_firsts,
                            (int)(V - 1), h->unigram, kUnigramTableSize, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
   dfree(d_counts);
@@ -280,7 +298,7 @@ fw2v_status fw2v_load_corpus(fw2v_handle* h, const int32_t* stream, int64_t stre
   if (!h || !stream || !chunk_off || stream_len < 1 || n_chunks < 1)
     return fail(h, FW2V_ERR_ARGUMENT, "load_corpus: empty corpus");
   if (h->V == 0) return fail(h, FW2V_ERR_STATE, "load_corpus before set_vocab");
-  if (h->cfg.threads > n_chunks)
+  if (h->cfg.threads > n_chunks || h->cfg.threads > 65535)
     return fail(h, FW2V_ERR_ARGUMENT, "load_corpus: threads (%d) > sentence chunks (%lld)", h->cfg.threads,
                 (long long)n_chunks);
   if (stream[stream_len - 1] != 0) return fail(h, FW2V_ERR_ARGUMENT, "load_corpus: stream must end with 0");
@@ -295,6 +313,7 @@ fw2v_status fw2v_load_corpus(fw2v_handle* h, const int32_t* stream, int64_t stre
     CK(h, dalloc(h->stream_ids, stream_len));
     CK(h, dalloc(h->chunk_off, n_chunks));
     CK(h, dalloc(h->kept_ids, stream_len));
+    CK(h, dalloc(h->kept_state, stream_len));
     CK(h, dalloc(h->kept_negs, (size_t)stream_len * std::max(K, 1)));
     CK(h, dalloc(h->ent_start, stream_len + 2 * (int64_t)T));
     CK(h, dalloc(h->ent_len, stream_len + 2 * (int64_t)T));
@@ -309,6 +328,13 @@ fw2v_status fw2v_load_corpus(fw2v_handle* h, const int32_t* stream, int64_t stre
   }
   h->stream_len = stream_len;
   h->n_chunks = n_chunks;
+  h->max_region = 0;
+  for (int s = 0; s < T; s++) {
+    int64_t first, end;
+    stream_range(n_chunks, T, s, &first, &end);
+    const int64_t region = (end < n_chunks ? chunk_off[end] : stream_len) - chunk_off[first];
+    h->max_region = std::max(h->max_region, region);
+  }
   CK(h, cudaMemcpyAsync(h->stream_ids, stream, stream_len * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaMemcpyAsync(h->chunk_off, chunk_off, n_chunks * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
   CK(h, launch_validate_ids(h->stream_ids, stream_len, h->V, h->error_flag, h->stream));
@@ -336,9 +362,12 @@ fw2v_status fw2v_sample_epoch(fw2v_handle* h) {
   p.stream_len = h->stream_len;
   p.chunk_off = h->chunk_off;
   p.n_chunks = h->n_chunks;
-  p.p_keep = h->p_keep;
+  p.vocab = h->V;
+  p.keep_thr = h->keep_thr;
   p.sample = h->cfg.sample;
   p.unigram = h->unigram;
+  p.jump_a = h->jump_a;
+  p.jump_c = h->jump_c;
   p.table_size = kUnigramTableSize;
   p.threads = h->cfg.threads;
   p.msl = h->cfg.msl;
@@ -353,13 +382,14 @@ fw2v_status fw2v_sample_epoch(fw2v_handle* h) {
   p.ent_len = h->ent_len;
   p.ent_alpha = h->ent_alpha;
   p.kept_ids = h->kept_ids;
+  p.kept_state = h->kept_state;
   p.kept_negs = h->kept_negs;
   p.n_entries = h->n_entries;
   p.n_kept = h->n_kept;
   p.words = h->words;
   p.error_flag = h->error_flag;
   CK(h, cudaEventRecord(h->ev[0], h->stream));
-  CK(h, launch_sampler(p, h->entry_prefix, h->stream));
+  CK(h, launch_sampler(p, h->max_region, h->entry_prefix, h->stream));
   CK(h, cudaEventRecord(h->ev[1], h->stream));
   h->sampled = true;
   return FW2V_OK;

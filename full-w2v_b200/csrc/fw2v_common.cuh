@@ -59,10 +59,13 @@ struct SamplerParams {
   int64_t stream_len;
   const int64_t* chunk_off;
   int64_t n_chunks;
-  const float* p_keep;
+  int64_t vocab;
+  const int32_t* keep_thr;  // keep a token iff (lcg & 0xFFFF) <= keep_thr[word]
   float sample;
   const int32_t* unigram;
   int64_t table_size;
+  const uint64_t* jump_a;   // r -> jump_a[m] * r + jump_c[m] is m LCG steps
+  const uint64_t* jump_c;
   int threads, msl, negative, epochs;
   float alpha0;
   uint64_t train_words;
@@ -75,6 +78,7 @@ struct SamplerParams {
   int32_t* ent_len;
   float* ent_alpha;
   int32_t* kept_ids;
+  uint64_t* kept_state;     // LCG state after a kept token's keep decision
   int32_t* kept_negs;
   int64_t* n_entries;
   int64_t* n_kept;

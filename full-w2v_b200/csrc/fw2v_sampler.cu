@@ -1,25 +1,41 @@
-// On-device batch builder: the sentence/subsampling/negative-sampling loop of
-// Train_SGNS (FULL-W2V-driver.cu:166-302), one CUDA thread per reference
-// "thread" (LCG stream).  Every stream owns a contiguous range of stored
-// chunks (FULL-W2V-driver.cu:103-110), an LCG seeded with its id (:114) that
-// persists across epochs, and its own learning-rate state.
+// On-device batch builder: the sentence / subsampling / negative-sampling loop
+// of Train_SGNS (FULL-W2V-driver.cu:166-302).  Every reference "thread" is a
+// sampling stream: a contiguous range of stored chunks (FULL-W2V-driver.cu:
+// 103-110) and an LCG seeded with its id (:114) that persists across epochs.
 //
-// Output of one epoch, per stream s:
-//   entries  ent_{start,len,alpha}[entry_base(s) + e], e < n_entries[s]
-//            (every batch entry the reference records, zero-length ones too)
-//   kept ids kept_ids[kept_base(s) + k], k < n_kept[s], and K negatives each
-//            at kept_negs[(kept_base(s) + k) * K + j]
+// The LCG chain of a stream is inherently serial (a kept token advances it by
+// 1+K steps, a dropped one by 1), but its decisions only depend on the low 16
+// bits of the state, and the low 32 bits of an LCG mod 2^64 form an LCG mod
+// 2^32 of their own.  So one warp runs a stream: the 32 lanes load 32 tokens
+// and their keep thresholds at once, then walk them in order with a 32-bit
+// state (one multiply-add per step, the K negatives' steps folded into one
+// precomputed K-step map).  Each lane records the step at which its own token
+// was kept; the full 64-bit state there follows from the state at the start of
+// the 32-token block by one jump-ahead multiply-add (table of r -> A_m r + C_m).
+// A second, fully parallel kernel turns each kept token's state into its K
+// negative ids (FULL-W2V-driver.cu:224-227).
+//
+// Output of one epoch, per stream s (kept_base(s) = chunk_off[first chunk],
+// entry_base(s) = kept_base(s) + 2s):
+//   entries  ent_{start,len,alpha}[entry_base(s) + e], e < n_entries[s]: every
+//            batch entry the reference records, zero-length ones included
+//   kept     kept_ids / kept_state[kept_base(s) + k], k < n_kept[s], and
+//            kept_negs[(kept_base(s) + k) * K + j]
 //   words[s] tokens read this epoch (EOS and subsampled-away tokens included).
-// kept_base(s) = chunk_off[first chunk of s]; entry_base(s) = kept_base(s) + 2s.
-// Capacities follow from the region of stream s in the token stream; a stream
-// that would overflow them (possible only with chunk tables whose chunks are
-// shorter than msl without a closing 0) stops and raises the error flag.
 #include "fw2v_common.cuh"
 
 namespace fw2v {
 
-__global__ void __launch_bounds__(128) sampler_epoch_kernel(SamplerParams p) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+namespace {
+
+constexpr uint32_t kLcgMul32 = (uint32_t)kLcgMul;
+constexpr uint32_t kLcgAdd32 = (uint32_t)kLcgAdd;
+
+}  // namespace
+
+__global__ void __launch_bounds__(128) sampler_warp_kernel(SamplerParams p) {
+  const int lane = threadIdx.x & 31;
+  const int s = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (s >= p.threads) return;
   int64_t es, ee;
   stream_range(p.n_chunks, p.threads, s, &es, &ee);
@@ -30,91 +46,150 @@ __global__ void __launch_bounds__(128) sampler_epoch_kernel(SamplerParams p) {
   const int64_t entry_cap = kept_cap + 2;
   const int K = p.negative;
   const int msl = p.msl;
+  const bool subsample = p.sample > 0.0f;
+  const uint32_t aK = (uint32_t)p.jump_a[K];
+  const uint32_t cK = (uint32_t)p.jump_c[K];
 
-  uint64_t lcg = p.lcg[s];
+  uint64_t r_blk = p.lcg[s];  // full state at the start of the current block
+  uint32_t r32 = (uint32_t)r_blk;
   uint64_t wca_own = p.wca_own[s];
   float alpha = p.alpha[s];
   uint64_t word_count = 0, last_word_count = 0;
-  int64_t ss = es, cur = 0;
-  int64_t ne = 0, nk = 0;
+  int64_t nk = 0, ne = 0;
+  int L = 0;
   bool fail = false;
 
-  for (;;) {
-    if (word_count - last_word_count > 10000) {
+  // Record a batch entry of `len` kept words, then the learning-rate refresh the
+  // reference performs before building the next sentence (FULL-W2V-driver.cu:168-190).
+  auto record = [&](int len, bool refresh) {
+    if (ne >= entry_cap) {
+      fail = true;
+      return;
+    }
+    if (lane == 0) {
+      p.ent_start[entry_b + ne] = kept_base + nk;
+      p.ent_len[entry_b + ne] = len;
+      p.ent_alpha[entry_b + ne] = alpha;
+    }
+    ne++;
+    nk += len;
+    if (refresh && word_count - last_word_count > 10000) {
       wca_own += word_count - last_word_count;
       last_word_count = word_count;
       alpha = refreshed_alpha(p.alpha0, wca_own, p.threads, p.epochs, p.train_words);
     }
-    int32_t L = 0;
-    while (L < msl) {
-      if (cur >= msl) {
-        ss++;
-        cur = 0;
-        if (ss >= ee) break;
+  };
+
+  for (int64_t ss = es; ss < ee && !fail; ss++) {
+    const int64_t off = p.chunk_off[ss];
+    bool chunk_done = false;
+    for (int cur0 = 0; cur0 < msl && !chunk_done && !fail; cur0 += 32) {
+      // A chunk is read from its start until msl tokens or its first 0 (EOS).
+      const int cur = cur0 + lane;
+      const int64_t pos = off + cur;
+      const bool inb = cur < msl && pos < p.stream_len;
+      const int w = inb ? __ldg(p.stream + pos) : -1;
+      const unsigned zmask = __ballot_sync(kFull, inb && w == 0);
+      int nvalid = msl - cur0 < 32 ? msl - cur0 : 32;
+      if (zmask) {
+        const int z = __ffs(zmask);
+        if (z < nvalid) nvalid = z;
       }
-      const int64_t pos = p.chunk_off[ss] + cur;
-      if (pos >= p.stream_len) {
+      const bool bad = lane < nvalid && (!inb || w < 0 || (int64_t)w >= p.vocab);
+      if (__any_sync(kFull, bad)) {
         fail = true;
         break;
       }
-      const int32_t w = __ldg(p.stream + pos);
-      cur++;
-      word_count++;
-      if (w == 0 || ss >= ee) {
-        ss++;
-        cur = 0;
-        break;
+      const int thr = (lane < nvalid && w > 0) ? __ldg(p.keep_thr + w) : 0;
+      bool my_keep = false;
+      int my_m = 0;
+      int64_t my_slot = 0;
+      int m = 0;  // LCG steps taken in this block
+      for (int i = 0; i < nvalid; i++) {
+        const int wi = __shfl_sync(kFull, w, i);
+        const int ti = __shfl_sync(kFull, thr, i);
+        word_count++;
+        if (wi == 0) {
+          // EOS ends the chunk; it ends the sentence unless it closes the
+          // stream's range, where the partial sentence is dropped (:233-247).
+          chunk_done = true;
+          if (ss + 1 < ee) {
+            record(L, true);
+            L = 0;
+          }
+          break;
+        }
+        bool keep = true;
+        if (subsample) {
+          r32 = r32 * kLcgMul32 + kLcgAdd32;
+          m++;
+          keep = (int)(r32 & 0xFFFFu) <= ti;
+        }
+        if (keep) {
+          if (lane == i) {
+            my_keep = true;
+            my_m = m;
+            my_slot = nk + L;
+          }
+          r32 = r32 * aK + cK;
+          m += K;
+          L++;
+          if (L == msl) {
+            record(L, true);
+            L = 0;
+          }
+        }
       }
-      if (p.sample > 0.0f) {
-        lcg = lcg_next(lcg);
-        const float u = __uint2float_rn((unsigned)(lcg & 0xFFFF)) / 65536.0f;
-        if (__ldg(p.p_keep + w) < u) continue;
+      bool lfail = false;
+      if (my_keep) {
+        if (my_slot >= kept_cap) {
+          lfail = true;
+        } else {
+          p.kept_ids[kept_base + my_slot] = w;
+          p.kept_state[kept_base + my_slot] = p.jump_a[my_m] * r_blk + p.jump_c[my_m];
+        }
       }
-      if (nk + L >= kept_cap) {
-        fail = true;
-        break;
-      }
-      const int64_t slot = kept_base + nk + L;
-      p.kept_ids[slot] = w;
-      for (int k = 0; k < K; k++) {
-        lcg = lcg_next(lcg);
-        const int64_t idx = (int64_t)((lcg >> 16) % (uint64_t)p.table_size);
-        p.kept_negs[slot * K + k] = __ldg(p.unigram + idx);
-      }
-      L++;
+      fail |= __any_sync(kFull, lfail);
+      r_blk = p.jump_a[m] * r_blk + p.jump_c[m];
     }
-    if (fail || ne >= entry_cap) {
-      fail = true;
-      break;
-    }
-    const int64_t e = entry_b + ne;
-    if (ss >= ee) {
-      // Epoch end (FULL-W2V-driver.cu:233-277): flush the count, drop the
-      // partial sentence (recorded with length 0).
-      wca_own += word_count - last_word_count;
-      p.ent_start[e] = kept_base + nk;
-      p.ent_len[e] = 0;
-      p.ent_alpha[e] = alpha;
-      ne++;
-      break;
-    }
-    p.ent_start[e] = kept_base + nk;
-    p.ent_len[e] = L;
-    p.ent_alpha[e] = alpha;
-    ne++;
-    nk += L;
+  }
+  if (!fail) {
+    // Epoch end (FULL-W2V-driver.cu:233-277): flush the count, drop the partial
+    // sentence (recorded with length 0).
+    wca_own += word_count - last_word_count;
+    record(0, false);
   }
   if (fail) {
-    atomicExch(p.error_flag, 1);
+    if (lane == 0) atomicExch(p.error_flag, 1);
     ne = 0;
     nk = 0;
   }
-  p.lcg[s] = lcg;
-  p.wca_own[s] = wca_own;
-  p.alpha[s] = alpha;
-  p.n_entries[s] = ne;
-  p.n_kept[s] = nk;
-  p.words[s] = word_count;
+  if (lane == 0) {
+    p.lcg[s] = r_blk;
+    p.wca_own[s] = wca_own;
+    p.alpha[s] = alpha;
+    p.n_entries[s] = ne;
+    p.n_kept[s] = nk;
+    p.words[s] = word_count;
+  }
+}
+
+// K negatives of every kept token from its LCG state: the reference draws them
+// right after the token's keep decision, one LCG step each, and indexes the
+// unigram table with (state >> 16) % table_size (FULL-W2V-driver.cu:224-227).
+__global__ void __launch_bounds__(256) negatives_kernel(SamplerParams p) {
+  const int s = blockIdx.y;
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= p.threads || k >= p.n_kept[s]) return;
+  int64_t es, ee;
+  stream_range(p.n_chunks, p.threads, s, &es, &ee);
+  const int64_t slot = p.chunk_off[es] + k;
+  uint64_t r = p.kept_state[slot];
+  int32_t* out = p.kept_negs + slot * p.negative;
+  for (int j = 0; j < p.negative; j++) {
+    r = lcg_next(r);
+    out[j] = __ldg(p.unigram + (int64_t)((r >> 16) % (uint64_t)p.table_size));
+  }
 }
 
 // Exclusive prefix sum of n_entries over streams (one block), so that the
@@ -143,10 +218,15 @@ __global__ void __launch_bounds__(1024) entry_prefix_kernel(const int64_t* n_ent
   if (t == 1023) prefix[threads] = partial[1023];
 }
 
-cudaError_t launch_sampler(const SamplerParams& p, int64_t* entry_prefix, cudaStream_t st) {
-  const int block = 128;
-  const int grid = (p.threads + block - 1) / block;
-  sampler_epoch_kernel<<<grid, block, 0, st>>>(p);
+cudaError_t launch_sampler(const SamplerParams& p, int64_t max_region, int64_t* entry_prefix,
+                           cudaStream_t st) {
+  const int warps_per_block = 4;
+  const int grid = (p.threads + warps_per_block - 1) / warps_per_block;
+  sampler_warp_kernel<<<grid, warps_per_block * 32, 0, st>>>(p);
+  if (p.negative > 0) {
+    const dim3 ngrid((unsigned)((max_region + 255) / 256), (unsigned)p.threads);
+    negatives_kernel<<<ngrid, 256, 0, st>>>(p);
+  }
   entry_prefix_kernel<<<1, 1024, 0, st>>>(p.n_entries, p.threads, entry_prefix);
   return cudaGetLastError();
 }

@@ -33,14 +33,18 @@ __global__ void init_syn0_kernel(float* syn0, int64_t V, int d, int64_t pitch) {
   }
 }
 
-// improved_driver_functions.cpp:71-77
+// improved_driver_functions.cpp:71-77, as an integer threshold: the reference
+// drops a token iff p < u/65536 (FULL-W2V-driver.cu:218), u = lcg & 0xFFFF;
+// p*65536 is exact in float, so it keeps iff u <= floor(p*65536).
 __global__ void subsample_kernel(const uint32_t* counts, int64_t V, float sample, uint64_t train_words,
-                                 float* p_keep) {
+                                 int32_t* keep_thr) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= V) return;
   const float base = __fmul_rn(sample, __ull2float_rn(train_words));
   const float ratio = __fdiv_rn(base, __uint2float_rn(counts[i]));
-  p_keep[i] = __fadd_rn(__fsqrt_rn(ratio), ratio);
+  const float pk = __fadd_rn(__fsqrt_rn(ratio), ratio);
+  const float scaled = __fmul_rn(pk, 65536.0f);
+  keep_thr[i] = (isnan(pk) || scaled >= 65535.0f) ? 65535 : (int32_t)floorf(scaled);
 }
 
 // firsts[j] = first table index of word j+1 (j < n), non-decreasing.
@@ -103,12 +107,12 @@ extern "C" int fw2v_unigram_firsts(const uint32_t* counts, int64_t V, int64_t si
 namespace fw2v {
 
 cudaError_t launch_init_tables(float* syn0, int64_t V, int d, int64_t pitch, const uint32_t* d_counts,
-                               float sample, uint64_t train_words, float* p_keep,
+                               float sample, uint64_t train_words, int32_t* keep_thr,
                                const int64_t* d_firsts, int n_firsts, int32_t* unigram,
                                int64_t table_size, cudaStream_t st) {
   const int b = 256;
   init_syn0_kernel<<<(unsigned)((V + b - 1) / b), b, 0, st>>>(syn0, V, d, pitch);
-  subsample_kernel<<<(unsigned)((V + b - 1) / b), b, 0, st>>>(d_counts, V, sample, train_words, p_keep);
+  subsample_kernel<<<(unsigned)((V + b - 1) / b), b, 0, st>>>(d_counts, V, sample, train_words, keep_thr);
   unigram_fill_kernel<<<148 * 16, 256, 0, st>>>(d_firsts, n_firsts, unigram, table_size);
   return cudaGetLastError();
 }
