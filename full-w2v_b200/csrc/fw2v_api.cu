@@ -22,7 +22,8 @@ cudaError_t launch_heldout(const TrainParams& p, double* loss, unsigned long lon
 cudaError_t launch_init_tables(float* syn0, int64_t V, int d, int64_t pitch, const uint32_t* d_counts,
                                float sample, uint64_t train_words, int32_t* keep_thr, const int64_t* d_firsts,
                                int n_firsts, int32_t* unigram, int64_t table_size, cudaStream_t st);
-size_t train_smem_bytes(int window, int64_t pitch, int warps);
+size_t train_smem_bytes(int window, int64_t pitch, int warps, int r);
+int64_t train_scratch_warps(int num_sms);
 cudaError_t launch_validate_ids(const int32_t* ids, int64_t n, int64_t vocab, int* flag, cudaStream_t st);
 }  // namespace fw2v
 
@@ -68,6 +69,8 @@ struct fw2v_handle {
 
   int* error_flag = nullptr;
   unsigned long long* work_counter = nullptr;
+  float* orig_scratch = nullptr;
+  int64_t scratch_warps = 0;
 
   bool sampled = false;
   int epochs_done = 0;
@@ -136,6 +139,8 @@ TrainParams base_train_params(fw2v_handle* h) {
   p.error_flag = h->error_flag;
   p.work_counter = h->work_counter;
   p.exp_table = h->exp_table;
+  p.orig_scratch = h->orig_scratch;
+  p.scratch_warps = h->scratch_warps;
   return p;
 }
 
@@ -208,7 +213,7 @@ fw2v_status fw2v_create(const fw2v_config* cfg, fw2v_handle** out) {
   if (cudaGetDeviceProperties(&prop, c.device) != cudaSuccess || prop.major != 10) return FW2V_ERR_NO_DEVICE;
   if (cudaSetDevice(c.device) != cudaSuccess) return FW2V_ERR_NO_DEVICE;
   const int64_t P = pitch_for(c.layer_size);
-  if (train_smem_bytes(c.window, P, 1) > (size_t)prop.sharedMemPerBlockOptin) return FW2V_ERR_ARGUMENT;
+  if (train_smem_bytes(c.window, P, 1, 8) > (size_t)prop.sharedMemPerBlockOptin) return FW2V_ERR_ARGUMENT;
   fw2v_handle* h = new fw2v_handle();
   h->cfg = c;
   h->num_sms = prop.multiProcessorCount;
@@ -222,6 +227,9 @@ fw2v_status fw2v_create(const fw2v_config* cfg, fw2v_handle** out) {
     if (cudaEventCreate(&e) != cudaSuccess) return cleanup(FW2V_ERR_CUDA);
   if (dalloc(h->error_flag, 1) != cudaSuccess || dalloc(h->work_counter, 1) != cudaSuccess ||
       dalloc(h->exp_table, kExpTableSize) != cudaSuccess)
+    return cleanup(FW2V_ERR_NOMEM);
+  h->scratch_warps = train_scratch_warps(h->num_sms);
+  if (dalloc(h->orig_scratch, (size_t)h->scratch_warps * (2 * c.window + 1) * P) != cudaSuccess)
     return cleanup(FW2V_ERR_NOMEM);
   // LCG jump-ahead table for up to 32 tokens of 1+K steps each.
   const int n_jump = 32 * (1 + c.negative) + 1;
@@ -256,7 +264,7 @@ void fw2v_destroy(fw2v_handle* h) {
   dfree(h->ent_start); dfree(h->ent_len); dfree(h->ent_alpha);
   dfree(h->kept_ids); dfree(h->kept_negs);
   dfree(h->n_entries); dfree(h->n_kept); dfree(h->words); dfree(h->entry_prefix);
-  dfree(h->error_flag); dfree(h->work_counter);
+  dfree(h->error_flag); dfree(h->work_counter); dfree(h->orig_scratch);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);

@@ -131,6 +131,10 @@ struct TrainParams {
   int deterministic;
   int* error_flag;
   const float* exp_table;
+  // per-warp scratch, (2W+1) * pitch floats for each of scratch_warps warps:
+  // the value every ring row had when it entered the window
+  float* orig_scratch;
+  int64_t scratch_warps;
 };
 
 __host__ __device__ __forceinline__ int64_t entry_base(const int64_t* chunk_off, int64_t n_chunks,

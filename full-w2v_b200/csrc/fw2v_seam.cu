@@ -15,7 +15,8 @@ extern "C" void fw2v_exp_table(float* t);
 
 namespace fw2v {
 cudaError_t launch_train(const TrainParams& p, int num_sms, cudaStream_t st);
-size_t train_smem_bytes(int window, int64_t pitch, int warps);
+size_t train_smem_bytes(int window, int64_t pitch, int warps, int r);
+int64_t train_scratch_warps(int num_sms);
 }  // namespace fw2v
 
 namespace {
@@ -85,8 +86,15 @@ extern "C" fw2v_status fw2v_kernel_batch(float* syn0, float* syn1neg, const int3
   p.error_flag = (int*)addr;
   if (cudaGetSymbolAddress(&addr, g_seam_exp_table) != cudaSuccess) return FW2V_ERR_CUDA;
   p.exp_table = (const float*)addr;
-  if (fw2v::launch_train(p, g_seam_sms[dev], (cudaStream_t)stream) != cudaSuccess) return FW2V_ERR_CUDA;
-  return FW2V_OK;
+  // Per-launch scratch from the stream-ordered allocator, so concurrent
+  // launches on different streams never share it.
+  cudaStream_t st = (cudaStream_t)stream;
+  p.scratch_warps = fw2v::train_scratch_warps(g_seam_sms[dev]);
+  const size_t bytes = (size_t)p.scratch_warps * (2 * window + 1) * pitch * sizeof(float);
+  if (cudaMallocAsync((void**)&p.orig_scratch, bytes, st) != cudaSuccess) return FW2V_ERR_NOMEM;
+  const cudaError_t e = fw2v::launch_train(p, g_seam_sms[dev], st);
+  cudaFreeAsync(p.orig_scratch, st);
+  return e == cudaSuccess ? FW2V_OK : FW2V_ERR_CUDA;
 }
 
 extern "C" fw2v_status fw2v_kernel_batch_error(void* stream) {

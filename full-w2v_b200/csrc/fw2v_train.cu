@@ -3,13 +3,21 @@
 
 namespace fw2v {
 
-extern template cudaError_t launch_r<2, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 2>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 3>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 4>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 6>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 8>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<2, 1, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<2, 1, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<4, 1, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<4, 1, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<4, 2, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<4, 2, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<4, 3, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<4, 3, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<4, 4, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<4, 4, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<4, 6, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<4, 6, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<4, 8, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<4, 8, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+
 
 struct LaunchShape {
   int vec, nv, r;
@@ -29,24 +37,31 @@ LaunchShape choose_shape(int d, int negative) {
   }
   const int want = negative + 1;
   s.r = want <= 1 ? 1 : want <= 2 ? 2 : want <= 4 ? 4 : want <= 6 ? 6 : 8;
+  if (s.nv >= 4) s.r = 1;
   return s;
 }
 
-size_t train_smem_bytes(int window, int64_t pitch, int warps) {
-  return (size_t)(1024 + (size_t)warps * 2 * (2 * window + 1) * pitch) * sizeof(float);
+// Shared memory of one block: per warp, the ring of 2W+1 rows, a sink row, R
+// target originals and two staging rows (WarpRows).
+size_t train_smem_bytes(int window, int64_t pitch, int warps, int r) {
+  return (size_t)warps * (2 * window + 1 + 3 + r) * pitch * sizeof(float);
 }
+
+// Warps the scratch of a handle must cover: every warp the persistent grid can
+// hold (64 per SM at most).
+int64_t train_scratch_warps(int num_sms) { return (int64_t)num_sms * 64; }
 
 cudaError_t launch_train(const TrainParams& p, int num_sms, cudaStream_t st) {
   const LaunchShape s = choose_shape(p.d, p.negative);
-  const size_t smem = train_smem_bytes(p.window, p.pitch, p.deterministic ? 1 : kWarpsPerBlock);
-  if (s.vec == 2) return launch_r<2, 1>(p, s.r, num_sms, smem, st);
+  const size_t smem = train_smem_bytes(p.window, p.pitch, p.deterministic ? 1 : kWarpsPerBlock, s.r);
+  if (s.vec == 2) return p.sigmoid == 0 ? launch_r<2, 1, 0>(p, s.r, num_sms, smem, st) : launch_r<2, 1, 1>(p, s.r, num_sms, smem, st);
   switch (s.nv) {
-    case 1: return launch_r<4, 1>(p, s.r, num_sms, smem, st);
-    case 2: return launch_r<4, 2>(p, s.r, num_sms, smem, st);
-    case 3: return launch_r<4, 3>(p, s.r, num_sms, smem, st);
-    case 4: return launch_r<4, 4>(p, s.r, num_sms, smem, st);
-    case 6: return launch_r<4, 6>(p, s.r, num_sms, smem, st);
-    default: return launch_r<4, 8>(p, s.r, num_sms, smem, st);
+    case 1: return p.sigmoid == 0 ? launch_r<4, 1, 0>(p, s.r, num_sms, smem, st) : launch_r<4, 1, 1>(p, s.r, num_sms, smem, st);
+    case 2: return p.sigmoid == 0 ? launch_r<4, 2, 0>(p, s.r, num_sms, smem, st) : launch_r<4, 2, 1>(p, s.r, num_sms, smem, st);
+    case 3: return p.sigmoid == 0 ? launch_r<4, 3, 0>(p, s.r, num_sms, smem, st) : launch_r<4, 3, 1>(p, s.r, num_sms, smem, st);
+    case 4: return p.sigmoid == 0 ? launch_r<4, 4, 0>(p, s.r, num_sms, smem, st) : launch_r<4, 4, 1>(p, s.r, num_sms, smem, st);
+    case 6: return p.sigmoid == 0 ? launch_r<4, 6, 0>(p, s.r, num_sms, smem, st) : launch_r<4, 6, 1>(p, s.r, num_sms, smem, st);
+    default: return p.sigmoid == 0 ? launch_r<4, 8, 0>(p, s.r, num_sms, smem, st) : launch_r<4, 8, 1>(p, s.r, num_sms, smem, st);
   }
 }
 

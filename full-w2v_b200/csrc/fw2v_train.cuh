@@ -32,15 +32,114 @@
 // are not reproduced.
 #pragma once
 #include <cstdio>
+#include <utility>
 
 #include "fw2v_common.cuh"
 
 namespace fw2v {
 
+// Compile-time loop: f(std::integral_constant<int, I>) for I = 0..N-1, so that
+// register arrays indexed by I are never indexed at run time.
+template <class F, int... Is>
+__device__ __forceinline__ void static_for_impl(F&& f, std::integer_sequence<int, Is...>) {
+  (f(std::integral_constant<int, Is>{}), ...);
+}
+template <int N, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+  static_for_impl(f, std::make_integer_sequence<int, N>{});
+}
+
 template <int VEC, int NV>
 struct Row {
   float x[NV][VEC];
 };
+
+// Shared-memory rows addressed by 32-bit shared-window byte offsets.  Lane l
+// accesses vector i of a row at byte offset lane_off(i) when lane_ok(i).
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+template <int VEC, int NV>
+struct LaneMap {
+  uint32_t off[NV];  // byte offset of this lane's vector i within a row
+  bool ok[NV];       // vector i starts inside the row (e < d)
+  __device__ __forceinline__ LaneMap(int lane, int d) {
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+      const int e = (i * 32 + lane) * VEC;
+      off[i] = (uint32_t)e * 4u;
+      ok[i] = e < d;
+    }
+  }
+};
+
+template <int VEC, int NV>
+__device__ __forceinline__ void lds_row(Row<VEC, NV>& r, uint32_t row, const LaneMap<VEC, NV>& m) {
+#pragma unroll
+  for (int i = 0; i < NV; i++) {
+    if constexpr (VEC == 4) {
+      float a = 0.f, b = 0.f, c = 0.f, e = 0.f;
+      if (m.ok[i])
+        asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
+                     : "=f"(a), "=f"(b), "=f"(c), "=f"(e)
+                     : "r"(row + m.off[i]));
+      r.x[i][0] = a; r.x[i][1] = b; r.x[i][2] = c; r.x[i][3] = e;
+    } else {
+      float a = 0.f, b = 0.f;
+      if (m.ok[i]) asm volatile("ld.shared.v2.f32 {%0,%1}, [%2];" : "=f"(a), "=f"(b) : "r"(row + m.off[i]));
+      r.x[i][0] = a; r.x[i][1] = b;
+    }
+  }
+}
+
+template <int VEC, int NV>
+__device__ __forceinline__ void sts_row(const Row<VEC, NV>& r, uint32_t row, const LaneMap<VEC, NV>& m) {
+#pragma unroll
+  for (int i = 0; i < NV; i++) {
+    if (m.ok[i]) {
+      if constexpr (VEC == 4) {
+        asm volatile("st.shared.v4.f32 [%0], {%1,%2,%3,%4};" ::"r"(row + m.off[i]), "f"(r.x[i][0]),
+                     "f"(r.x[i][1]), "f"(r.x[i][2]), "f"(r.x[i][3])
+                     : "memory");
+      } else {
+        asm volatile("st.shared.v2.f32 [%0], {%1,%2};" ::"r"(row + m.off[i]), "f"(r.x[i][0]), "f"(r.x[i][1])
+                     : "memory");
+      }
+    }
+  }
+}
+
+// Global -> shared copy of this lane's part of a row without a register
+// round trip (cp.async, 16 or 8 bytes per vector); complete with cp_async_wait.
+template <int VEC, int NV>
+__device__ __forceinline__ void cp_row(uint32_t dst, const float* src, const LaneMap<VEC, NV>& m, int d) {
+#pragma unroll
+  for (int i = 0; i < NV; i++) {
+    if (m.ok[i]) {
+      const float* g = src + m.off[i] / 4;
+      if ((int)(m.off[i] / 4) + VEC <= d) {
+        if constexpr (VEC == 4)
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + m.off[i]), "l"(g) : "memory");
+        else
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst + m.off[i]), "l"(g) : "memory");
+      } else {
+        // a vector that straddles d: element copies, zeros past d
+#pragma unroll
+        for (int j = 0; j < VEC; j++) {
+          const int e = (int)(m.off[i] / 4) + j;
+          if (e < d)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst + m.off[i] + 4 * j), "l"(g + j)
+                         : "memory");
+          else
+            asm volatile("st.shared.f32 [%0], %1;" ::"r"(dst + m.off[i] + 4 * j), "f"(0.0f) : "memory");
+        }
+      }
+    }
+  }
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 template <int VEC, int NV>
 __device__ __forceinline__ void row_zero(Row<VEC, NV>& r) {
@@ -167,12 +266,12 @@ __device__ __forceinline__ void row_update(Row<VEC, NV>& v, Row<VEC, NV>& o, flo
 // alpha * (label - sigma(x)).  Table mode reproduces FULL-W2V-kernels.cu:92-99:
 // index = (int)(saturate((x + 6) / 12) * 999); the positive target reads the
 // reversed table (nexpTable[i] == expTable[999 - i]).
-__device__ __forceinline__ float gradient(float x, bool positive, float alpha, int sigmoid,
-                                          const float* table) {
-  if (sigmoid == 0) {
+template <int SIG>
+__device__ __forceinline__ float gradient(float x, bool positive, float alpha, const float* table) {
+  if constexpr (SIG == 0) {
     const float s = __saturatef(__fmul_rn(__fadd_rn(x, 6.0f), 1.0f / 12.0f));
     const int idx = __float2int_rz(__fmul_rn(s, 999.0f));
-    return positive ? __fmul_rn(alpha, table[kExpTableSize - 1 - idx]) : __fmul_rn(-alpha, table[idx]);
+    return positive ? __fmul_rn(alpha, __ldg(table + (kExpTableSize - 1 - idx))) : __fmul_rn(-alpha, __ldg(table + idx));
   }
   return positive ? __fdiv_rn(alpha, __fadd_rn(1.0f, expf(x)))
                   : __fdiv_rn(-alpha, __fadd_rn(1.0f, expf(-x)));
@@ -286,8 +385,39 @@ __device__ __forceinline__ int target_id(const int32_t* ids, const int32_t* negs
   return k == 0 ? __ldg(ids + w) : __ldg(negs + (int64_t)w * K + (k - 1));
 }
 
-template <int VEC, int NV, int R>
-__device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* ring_cur, float* ring_orig,
+template <int VEC, int NV>
+__device__ __forceinline__ void row_store_global(const Row<VEC, NV>& r, float* row, int lane, int d) {
+#pragma unroll
+  for (int i = 0; i < NV; i++) {
+    const int e = (i * 32 + lane) * VEC;
+    if (e < d) {
+      if constexpr (VEC == 4) {
+        __stcg(reinterpret_cast<float4*>(row + e), make_float4(r.x[i][0], r.x[i][1], r.x[i][2], r.x[i][3]));
+      } else {
+        __stcg(reinterpret_cast<float2*>(row + e), make_float2(r.x[i][0], r.x[i][1]));
+      }
+    }
+  }
+}
+
+// Shared-memory rows of one warp, each `P` floats.
+template <int R>
+struct WarpRows {
+  static constexpr int kExtra = 1 + R + 2;  // sink, R target originals, 2 staging rows
+  __host__ __device__ static constexpr int rows(int D) { return D + kExtra; }
+};
+
+// One sentence on one warp.
+//   ring     shared memory (WarpRows<R>::rows(D) rows): slot p % D holds the
+//            current value of sentence position p while it is in the window;
+//            slot D is a sink that the pipeline reads and writes on its idle
+//            steps; then the R target rows as loaded (for their write-back) and
+//            two staging rows filled by cp.async (the entering row and the
+//            leaving row's original value).
+//   orig     this warp's global scratch, D rows: the value each slot's row had
+//            when it entered the window (needed for its single write-back).
+template <int VEC, int NV, int R, int SIG>
+__device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* ring, float* orig,
                                const float* table, int lane) {
   constexpr int RP = PadPow2<R>::value;
   const int W = p.window, K = p.negative, D = 2 * W + 1;
@@ -296,6 +426,8 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   const int L = sn.len;
   const int32_t* ids = p.ids + sn.start;
   const int32_t* negs = p.negs + sn.start * (int64_t)K;
+  float* const syn0 = p.syn0;
+  float* const syn1neg = p.syn1neg;
   const float alpha = sn.alpha;
   const bool one_group = K + 1 <= R;
 
@@ -318,35 +450,44 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   Row<VEC, NV> tmp;
   const int n_enter = W + 1 < L ? W + 1 : L;
   for (int q = 0; q < n_enter; q++) {
-    row_load_global(tmp, p.syn0 + (int64_t)__ldg(ids + q) * P, lane, d);
-    row_store_smem(tmp, ring_cur + q * P, lane, d);
-    row_store_smem(tmp, ring_orig + q * P, lane, d);
+    row_load_global(tmp, syn0 + (int64_t)__ldg(ids + q) * P, lane, d);
+    row_store_smem(tmp, ring + q * P, lane, d);
+    row_store_global(tmp, orig + q * P, lane, d);
   }
+  const LaneMap<VEC, NV> lm(lane, d);
+  const uint32_t ring_b = smem_addr(ring);
+  const uint32_t row_bytes = (uint32_t)P * 4u;
+  const uint32_t sink_b = ring_b + (uint32_t)D * row_bytes;
+  const uint32_t o0_b = sink_b + row_bytes;
+  const uint32_t in_b = o0_b + (uint32_t)R * row_bytes;
+  const uint32_t out_b = in_b + row_bytes;
 
   // v[r] holds the context row whose index j in the centre's list has
   // j % R == r: stage k works on context t-k at step t, i.e. on register slot
   // (t - k) % R, so a row moves from stage to stage without being copied.
-  Row<VEC, NV> v[R], o[R], o0[R];
-  int vslot[R];
+  Row<VEC, NV> v[R], o[R];
+  uint32_t voff[R];
 #pragma unroll
   for (int k = 0; k < R; k++) {
     row_zero(v[k]);
-    vslot[k] = 0;
+    voff[k] = sink_b;
   }
 
   int t_next = one_group ? target_id(ids, negs, K, 0, 0, K + 1, lane) : 0;
   for (int w = 0; w < L; w++) {
-    // Ids needed later in this centre, loaded ahead of use.
+    // Ids and rows needed later in this centre, loaded ahead of use.
     const int q_out = w - W, q_in = w + W + 1;
     const int id_out = q_out >= 0 ? __ldg(ids + q_out) : -1;
     const int id_in = q_in < L ? __ldg(ids + q_in) : -1;
     const int t_here = t_next;
     if (one_group && w + 1 < L) t_next = target_id(ids, negs, K, w + 1, 0, K + 1, lane);
     // The entering row can be fetched now unless the leaving position holds
-    // the same word (its write-back must land first).
+    // the same word (its write-back must land first).  Both staging copies run
+    // in the background while the centre trains.
     const bool enter_early = id_in >= 0 && id_in != id_out;
-    Row<VEC, NV> enter_row;
-    if (enter_early) row_load_global(enter_row, p.syn0 + (int64_t)id_in * P, lane, d);
+    if (enter_early) cp_row(in_b, syn0 + (int64_t)id_in * P, lm, d);
+    if (q_out >= 0) cp_row(out_b, orig + (q_out % D) * P, lm, d);
+    cp_async_commit();
 
     // Lane r < D decides whether ring slot r holds a context of centre w.
     const int base = w - W;
@@ -370,129 +511,145 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
         }
         if (!__any_sync(kFull, dup)) {
           // ---- pipelined sweeps of nt targets ----
-          int t[R];
 #pragma unroll
           for (int k = 0; k < R; k++) {
-            t[k] = __shfl_sync(kFull, my_t, k);
+            const int tk = __shfl_sync(kFull, my_t, k);
             if (k < nt) {
-              row_load_global(o[k], p.syn1neg + (int64_t)t[k] * P, lane, d);
-              o0[k] = o[k];
+              row_load_global(o[k], syn1neg + (int64_t)tk * P, lane, d);
+              sts_row(o[k], o0_b + (uint32_t)k * row_bytes, lm);
             } else {
               row_zero(o[k]);
             }
           }
           const int my_stage = stage_of_lane<RP>(lane);
           const bool my_positive = k0 + my_stage == 0;
+          // the lane's stage is active at steps [my_stage, my_stage + nctx)
+          const unsigned my_span = my_stage < nt ? (unsigned)nctx : 0u;
           unsigned rem = mask;
           const int steps = nctx + R - 1;
           for (int t0 = 0; t0 < steps; t0 += R) {
-#pragma unroll
-            for (int u = 0; u < R; u++) {
+            static_for<R>([&](auto uc) {
+              constexpr int u = decltype(uc)::value;
               const int ts = t0 + u;
               if (ts < steps) {
-                if (ts < nctx) {
-                  const int s0 = __ffs(rem) - 1;
-                  rem &= rem - 1;
-                  vslot[u] = s0;
-                  row_load_smem(v[u], ring_cur + s0 * P, lane, d);
-                } else {
-                  row_zero(v[u]);
-                }
+                // stage 0 takes the next context (the sink once they run out);
+                // stage R-1 hands its row back (to the sink while ramping up)
+                const int s0 = __ffs(rem) - 1;
+                rem &= rem - 1;
+                voff[u] = s0 >= 0 ? ring_b + (uint32_t)s0 * row_bytes : sink_b;
+                lds_row(v[u], voff[u], lm);
                 float x[RP];
-#pragma unroll
-                for (int k = 0; k < RP; k++) x[k] = k < R ? row_dot(v[(u - k + R) % R], o[k < R ? k : 0]) : 0.0f;
+                static_for<RP>([&](auto kc) {
+                  constexpr int k = decltype(kc)::value;
+                  if constexpr (k < R) x[k] = row_dot(v[(u - k + R) % R], o[k]);
+                  else x[k] = 0.0f;
+                });
                 const float xs = transpose_reduce<RP>(x, lane);
-                const int j = ts - my_stage;
-                const bool act = my_stage < nt && j >= 0 && j < nctx;
-                const float g = act ? gradient(xs, my_positive, alpha, p.sigmoid, table) : 0.0f;
-#pragma unroll
-                for (int k = 0; k < R; k++) {
+                const bool act = (unsigned)(ts - my_stage) < my_span;
+                const float g = act ? gradient<SIG>(xs, my_positive, alpha, table) : 0.0f;
+                static_for<R>([&](auto kc) {
+                  constexpr int k = decltype(kc)::value;
                   const float gk = __shfl_sync(kFull, g, lane_of_stage<RP>(k));
                   row_update(v[(u - k + R) % R], o[k], gk);
-                }
-                const int jo = ts - (R - 1);
-                if (jo >= 0 && jo < nctx) row_store_smem(v[(u + 1) % R], ring_cur + vslot[(u + 1) % R] * P, lane, d);
+                });
+                constexpr int out = (u + 1) % R;
+                sts_row(v[out], voff[out], lm);
+                voff[out] = sink_b;
               }
-            }
+            });
           }
 #pragma unroll
-          for (int k = 0; k < R; k++)
-            if (k < nt) row_add_delta(p.syn1neg + (int64_t)t[k] * P, o[k], o0[k], lane, d);
+          for (int k = 0; k < R; k++) {
+            const int tk = __shfl_sync(kFull, my_t, k);
+            if (k < nt) {
+              Row<VEC, NV> o0;
+              lds_row(o0, o0_b + (uint32_t)k * row_bytes, lm);
+              row_add_delta(syn1neg + (int64_t)tk * P, o[k], o0, lane, d);
+            }
+          }
         } else {
           // ---- serial sweeps: a repeated target must see the earlier write ----
           for (int k = 0; k < nt; k++) {
             const int tk = __shfl_sync(kFull, my_t, k);
             Row<VEC, NV> so, so0, sv;
-            row_load_global(so, p.syn1neg + (int64_t)tk * P, lane, d);
+            row_load_global(so, syn1neg + (int64_t)tk * P, lane, d);
             so0 = so;
             unsigned rem = mask;
             for (int j = 0; j < nctx; j++) {
               const int s0 = __ffs(rem) - 1;
               rem &= rem - 1;
-              row_load_smem(sv, ring_cur + s0 * P, lane, d);
+              const uint32_t a = ring_b + (uint32_t)s0 * row_bytes;
+              lds_row(sv, a, lm);
               const float x = warp_sum(row_dot(sv, so));
-              const float g = gradient(x, k0 + k == 0, alpha, p.sigmoid, table);
+              const float g = gradient<SIG>(x, k0 + k == 0, alpha, table);
               row_update(sv, so, g);
-              row_store_smem(sv, ring_cur + s0 * P, lane, d);
+              sts_row(sv, a, lm);
             }
-            row_add_delta(p.syn1neg + (int64_t)tk * P, so, so0, lane, d);
+            row_add_delta(syn1neg + (int64_t)tk * P, so, so0, lane, d);
           }
         }
       }
     }
 
     // Slide the window: position w-W leaves, position w+W+1 takes its slot.
+    cp_async_wait();
     if (q_out >= 0) {
-      const int s = q_out % D;
       Row<VEC, NV> cur, org;
-      row_load_smem(cur, ring_cur + s * P, lane, d);
-      row_load_smem(org, ring_orig + s * P, lane, d);
-      row_add_delta(p.syn0 + (int64_t)id_out * P, cur, org, lane, d);
+      lds_row(cur, ring_b + (uint32_t)(q_out % D) * row_bytes, lm);
+      lds_row(org, out_b, lm);
+      row_add_delta(syn0 + (int64_t)id_out * P, cur, org, lane, d);
     }
     if (id_in >= 0) {
       const int s = q_in % D;
-      if (!enter_early) row_load_global(enter_row, p.syn0 + (int64_t)id_in * P, lane, d);
-      row_store_smem(enter_row, ring_cur + s * P, lane, d);
-      row_store_smem(enter_row, ring_orig + s * P, lane, d);
+      Row<VEC, NV> enter_row;
+      if (enter_early) lds_row(enter_row, in_b, lm);
+      else row_load_global(enter_row, syn0 + (int64_t)id_in * P, lane, d);
+      sts_row(enter_row, ring_b + (uint32_t)s * row_bytes, lm);
+      row_store_global(enter_row, orig + s * P, lane, d);
     }
   }
   // Positions still in the window leave in increasing order.
   for (int q = L - W > 0 ? L - W : 0; q < L; q++) {
     const int s = q % D;
     Row<VEC, NV> cur, org;
-    row_load_smem(cur, ring_cur + s * P, lane, d);
-    row_load_smem(org, ring_orig + s * P, lane, d);
-    row_add_delta(p.syn0 + (int64_t)__ldg(ids + q) * P, cur, org, lane, d);
+    lds_row(cur, ring_b + (uint32_t)s * row_bytes, lm);
+    row_load_global(org, orig + s * P, lane, d);
+    row_add_delta(syn0 + (int64_t)__ldg(ids + q) * P, cur, org, lane, d);
   }
 }
 
-template <int VEC, int NV, int R>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) sgns_train_kernel(TrainParams p) {
+// Blocks per SM the register budget is sized for: the one-vector shapes fit
+// 4 blocks (<= 128 registers); wider rows keep their stage registers with 2.
+template <int NV>
+struct MinBlocks {
+  static constexpr int value = NV == 1 ? 4 : 2;
+};
+
+template <int VEC, int NV, int R, int SIG>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, MinBlocks<NV>::value) sgns_train_kernel(TrainParams p) {
   extern __shared__ __align__(16) float smem[];
-  float* table = smem;
-  for (int i = threadIdx.x; i < kExpTableSize; i += blockDim.x) table[i] = p.exp_table[i];
-  __syncthreads();
+  const float* table = p.exp_table;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int D = 2 * p.window + 1;
-  const int64_t ring = (int64_t)D * p.pitch;
-  float* ring_cur = smem + 1024 + (int64_t)warp * 2 * ring;
-  float* ring_orig = ring_cur + ring;
+  float* ring = smem + (int64_t)warp * WarpRows<R>::rows(D) * p.pitch;
+  const int64_t gwarp = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+  float* orig = p.orig_scratch + gwarp * D * p.pitch;
   const int64_t total = total_sentences(p);
   if (p.deterministic) {
     if (blockIdx.x != 0 || warp != 0) return;
     for (int64_t w = 0; w < total; w++) {
       const Sentence sn = fetch_sentence(p, w);
-      train_sentence<VEC, NV, R>(p, sn, ring_cur, ring_orig, table, lane);
+      train_sentence<VEC, NV, R, SIG>(p, sn, ring, orig, table, lane);
     }
     return;
   }
   if (p.work_counter == nullptr) {
     // Static assignment (the kernel seam, whose launches may run concurrently).
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t w = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp; w < total; w += warps) {
+    for (int64_t w = gwarp; w < total; w += warps) {
       const Sentence sn = fetch_sentence(p, w);
-      train_sentence<VEC, NV, R>(p, sn, ring_cur, ring_orig, table, lane);
+      train_sentence<VEC, NV, R, SIG>(p, sn, ring, orig, table, lane);
     }
     return;
   }
@@ -502,7 +659,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) sgns_train_kernel(TrainPa
     w = __shfl_sync(kFull, w, 0);
     if ((int64_t)w >= total) break;
     const Sentence sn = fetch_sentence(p, (int64_t)w);
-    train_sentence<VEC, NV, R>(p, sn, ring_cur, ring_orig, table, lane);
+    train_sentence<VEC, NV, R, SIG>(p, sn, ring, orig, table, lane);
   }
 }
 
@@ -565,9 +722,9 @@ __global__ void __launch_bounds__(128) heldout_loss_kernel(TrainParams p, double
 
 // Launch of one (VEC, NV) shape for any stage count R (instantiated per shape
 // in fw2v_train_<shape>.cu so the shapes compile in parallel).
-template <int VEC, int NV, int R>
+template <int VEC, int NV, int R, int SIG>
 cudaError_t launch_t(const TrainParams& p, int num_sms, size_t smem, cudaStream_t st) {
-  auto kern = sgns_train_kernel<VEC, NV, R>;
+  auto kern = sgns_train_kernel<VEC, NV, R, SIG>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int blocks = 1;
@@ -580,19 +737,28 @@ cudaError_t launch_t(const TrainParams& p, int num_sms, size_t smem, cudaStream_
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     blocks = per_sm * num_sms;
+    const int64_t cap = p.scratch_warps / kWarpsPerBlock;
+    if (blocks > cap) blocks = (int)cap;
+    if (blocks < 1) return cudaErrorInvalidConfiguration;
   }
   kern<<<blocks, threads, smem, st>>>(p);
   return cudaGetLastError();
 }
 
-template <int VEC, int NV>
+// Stage counts compiled per shape: rows of up to 3 vectors per lane pipeline
+// up to 8 targets; wider rows (d > 384) sweep targets one at a time.
+template <int VEC, int NV, int SIG>
 cudaError_t launch_r(const TrainParams& p, int r, int num_sms, size_t smem, cudaStream_t st) {
-  switch (r) {
-    case 1: return launch_t<VEC, NV, 1>(p, num_sms, smem, st);
-    case 2: return launch_t<VEC, NV, 2>(p, num_sms, smem, st);
-    case 4: return launch_t<VEC, NV, 4>(p, num_sms, smem, st);
-    case 6: return launch_t<VEC, NV, 6>(p, num_sms, smem, st);
-    default: return launch_t<VEC, NV, 8>(p, num_sms, smem, st);
+  if constexpr (NV >= 4) {
+    return launch_t<VEC, NV, 1, SIG>(p, num_sms, smem, st);
+  } else {
+    switch (r) {
+      case 1: return launch_t<VEC, NV, 1, SIG>(p, num_sms, smem, st);
+      case 2: return launch_t<VEC, NV, 2, SIG>(p, num_sms, smem, st);
+      case 4: return launch_t<VEC, NV, 4, SIG>(p, num_sms, smem, st);
+      case 6: return launch_t<VEC, NV, 6, SIG>(p, num_sms, smem, st);
+      default: return launch_t<VEC, NV, 8, SIG>(p, num_sms, smem, st);
+    }
   }
 }
 
