@@ -29,6 +29,23 @@ cudaError_t launch_validate_ids(const int32_t* ids, int64_t n, int64_t vocab, in
 
 using namespace fw2v;
 
+struct SampleBuf {
+  int64_t* ent_start = nullptr;
+  int32_t* ent_len = nullptr;
+  float* ent_alpha = nullptr;
+  int32_t* kept_ids = nullptr;
+  uint64_t* kept_state = nullptr;
+  int32_t* kept_negs = nullptr;
+  int64_t* n_entries = nullptr;
+  int64_t* n_kept = nullptr;
+  uint64_t* words = nullptr;
+  int64_t* entry_prefix = nullptr;
+  cudaEvent_t start = nullptr;  // sampler launched
+  cudaEvent_t ready = nullptr;  // sampler outputs complete
+  cudaEvent_t freed = nullptr;  // trainer done reading them
+  bool used = false;            // `freed` has been recorded at least once
+};
+
 struct fw2v_handle {
   fw2v_config cfg{};
   int num_sms = 0;
@@ -56,23 +73,18 @@ struct fw2v_handle {
   uint64_t* lcg = nullptr;
   uint64_t* wca = nullptr;
   float* alpha = nullptr;
-  int64_t* ent_start = nullptr;
-  int32_t* ent_len = nullptr;
-  float* ent_alpha = nullptr;
-  int32_t* kept_ids = nullptr;
-  uint64_t* kept_state = nullptr;
-  int32_t* kept_negs = nullptr;
-  int64_t* n_entries = nullptr;
-  int64_t* n_kept = nullptr;
-  uint64_t* words = nullptr;
-  int64_t* entry_prefix = nullptr;
+  // Two sets of sampler outputs: epoch e is sampled into buf[e % 2] on the
+  // sampler stream while epoch e-1 trains from the other set.
+  SampleBuf buf[2];
+  cudaStream_t sstream = nullptr;
+  int64_t n_sampled = 0;  // epochs sampled since load_corpus
+  int64_t n_trained = 0;  // epochs trained since load_corpus
 
   int* error_flag = nullptr;
   unsigned long long* work_counter = nullptr;
   float* orig_scratch = nullptr;
   int64_t scratch_warps = 0;
 
-  bool sampled = false;
   int epochs_done = 0;
   uint64_t words_total = 0;
 };
@@ -223,8 +235,12 @@ fw2v_status fw2v_create(const fw2v_config* cfg, fw2v_handle** out) {
     return s;
   };
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return cleanup(FW2V_ERR_CUDA);
+  if (cudaStreamCreateWithFlags(&h->sstream, cudaStreamNonBlocking) != cudaSuccess) return cleanup(FW2V_ERR_CUDA);
   for (auto& e : h->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return cleanup(FW2V_ERR_CUDA);
+  for (SampleBuf& b : h->buf)
+    for (cudaEvent_t* e : {&b.start, &b.ready, &b.freed})
+      if (cudaEventCreate(e) != cudaSuccess) return cleanup(FW2V_ERR_CUDA);
   if (dalloc(h->error_flag, 1) != cudaSuccess || dalloc(h->work_counter, 1) != cudaSuccess ||
       dalloc(h->exp_table, kExpTableSize) != cudaSuccess)
     return cleanup(FW2V_ERR_NOMEM);
@@ -258,12 +274,18 @@ void fw2v_destroy(fw2v_handle* h) {
   cudaSetDevice(h->cfg.device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   dfree(h->syn0); dfree(h->syn1neg); dfree(h->keep_thr); dfree(h->unigram); dfree(h->exp_table);
-  dfree(h->jump_a); dfree(h->jump_c); dfree(h->kept_state);
+  dfree(h->jump_a); dfree(h->jump_c);
   dfree(h->stream_ids); dfree(h->chunk_off);
+  if (h->sstream) cudaStreamSynchronize(h->sstream);
   dfree(h->lcg); dfree(h->wca); dfree(h->alpha);
-  dfree(h->ent_start); dfree(h->ent_len); dfree(h->ent_alpha);
-  dfree(h->kept_ids); dfree(h->kept_negs);
-  dfree(h->n_entries); dfree(h->n_kept); dfree(h->words); dfree(h->entry_prefix);
+  for (SampleBuf& b : h->buf) {
+    dfree(b.ent_start); dfree(b.ent_len); dfree(b.ent_alpha);
+    dfree(b.kept_ids); dfree(b.kept_state); dfree(b.kept_negs);
+    dfree(b.n_entries); dfree(b.n_kept); dfree(b.words); dfree(b.entry_prefix);
+    for (cudaEvent_t* e : {&b.start, &b.ready, &b.freed})
+      if (*e) cudaEventDestroy(*e);
+  }
+  if (h->sstream) cudaStreamDestroy(h->sstream);
   dfree(h->error_flag); dfree(h->work_counter); dfree(h->orig_scratch);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
@@ -297,7 +319,7 @@ fw2v_status fw2v_set_vocab(fw2v_handle* h, const uint32_t* counts, int64_t V, ui
   CK(h, cudaStreamSynchronize(h->stream));
   dfree(d_counts);
   dfree(d_firsts);
-  h->sampled = false;
+  h->n_sampled = h->n_trained = 0;
   return FW2V_OK;
 }
 
@@ -317,22 +339,28 @@ fw2v_status fw2v_load_corpus(fw2v_handle* h, const int32_t* stream, int64_t stre
   CK(h, cudaSetDevice(h->cfg.device));
   const int T = h->cfg.threads;
   const int K = h->cfg.negative;
+  // Nothing may still read the previous corpus.
+  CK(h, cudaStreamSynchronize(h->sstream));
+  CK(h, cudaStreamSynchronize(h->stream));
   if (stream_len != h->stream_len || n_chunks != h->n_chunks || !h->stream_ids) {
     CK(h, dalloc(h->stream_ids, stream_len));
     CK(h, dalloc(h->chunk_off, n_chunks));
-    CK(h, dalloc(h->kept_ids, stream_len));
-    CK(h, dalloc(h->kept_state, stream_len));
-    CK(h, dalloc(h->kept_negs, (size_t)stream_len * std::max(K, 1)));
-    CK(h, dalloc(h->ent_start, stream_len + 2 * (int64_t)T));
-    CK(h, dalloc(h->ent_len, stream_len + 2 * (int64_t)T));
-    CK(h, dalloc(h->ent_alpha, stream_len + 2 * (int64_t)T));
+    for (SampleBuf& b : h->buf) {
+      CK(h, dalloc(b.kept_ids, stream_len));
+      CK(h, dalloc(b.kept_state, stream_len));
+      CK(h, dalloc(b.kept_negs, (size_t)stream_len * std::max(K, 1)));
+      CK(h, dalloc(b.ent_start, stream_len + 2 * (int64_t)T));
+      CK(h, dalloc(b.ent_len, stream_len + 2 * (int64_t)T));
+      CK(h, dalloc(b.ent_alpha, stream_len + 2 * (int64_t)T));
+      CK(h, dalloc(b.n_entries, T));
+      CK(h, dalloc(b.n_kept, T));
+      CK(h, dalloc(b.words, T));
+      CK(h, dalloc(b.entry_prefix, T + 1));
+      b.used = false;
+    }
     CK(h, dalloc(h->lcg, T));
     CK(h, dalloc(h->wca, T));
     CK(h, dalloc(h->alpha, T));
-    CK(h, dalloc(h->n_entries, T));
-    CK(h, dalloc(h->n_kept, T));
-    CK(h, dalloc(h->words, T));
-    CK(h, dalloc(h->entry_prefix, T + 1));
   }
   h->stream_len = stream_len;
   h->n_chunks = n_chunks;
@@ -355,7 +383,7 @@ fw2v_status fw2v_load_corpus(fw2v_handle* h, const int32_t* stream, int64_t stre
   CK(h, cudaMemcpyAsync(h->alpha, alpha.data(), T * sizeof(float), cudaMemcpyHostToDevice, h->stream));
   fw2v_status s = check_flag(h, "load_corpus");
   if (s != FW2V_OK) return s;
-  h->sampled = false;
+  h->n_sampled = h->n_trained = 0;
   h->epochs_done = 0;
   h->words_total = 0;
   return FW2V_OK;
@@ -364,7 +392,9 @@ fw2v_status fw2v_load_corpus(fw2v_handle* h, const int32_t* stream, int64_t stre
 fw2v_status fw2v_sample_epoch(fw2v_handle* h) {
   if (!h) return FW2V_ERR_ARGUMENT;
   if (!h->stream_ids || h->V == 0) return fail(h, FW2V_ERR_STATE, "sample_epoch before load_corpus");
+  if (h->n_sampled - h->n_trained >= 2) return fail(h, FW2V_ERR_STATE, "two sampled epochs are waiting to be trained");
   CK(h, cudaSetDevice(h->cfg.device));
+  SampleBuf& b = h->buf[h->n_sampled % 2];
   SamplerParams p{};
   p.stream = h->stream_ids;
   p.stream_len = h->stream_len;
@@ -386,54 +416,69 @@ fw2v_status fw2v_sample_epoch(fw2v_handle* h) {
   p.lcg = h->lcg;
   p.wca_own = h->wca;
   p.alpha = h->alpha;
-  p.ent_start = h->ent_start;
-  p.ent_len = h->ent_len;
-  p.ent_alpha = h->ent_alpha;
-  p.kept_ids = h->kept_ids;
-  p.kept_state = h->kept_state;
-  p.kept_negs = h->kept_negs;
-  p.n_entries = h->n_entries;
-  p.n_kept = h->n_kept;
-  p.words = h->words;
+  p.ent_start = b.ent_start;
+  p.ent_len = b.ent_len;
+  p.ent_alpha = b.ent_alpha;
+  p.kept_ids = b.kept_ids;
+  p.kept_state = b.kept_state;
+  p.kept_negs = b.kept_negs;
+  p.n_entries = b.n_entries;
+  p.n_kept = b.n_kept;
+  p.words = b.words;
   p.error_flag = h->error_flag;
-  CK(h, cudaEventRecord(h->ev[0], h->stream));
-  CK(h, launch_sampler(p, h->max_region, h->entry_prefix, h->stream));
-  CK(h, cudaEventRecord(h->ev[1], h->stream));
-  h->sampled = true;
+  // The set is reused two epochs later: wait until that epoch's trainer is done.
+  if (b.used) CK(h, cudaStreamWaitEvent(h->sstream, b.freed, 0));
+  CK(h, cudaEventRecord(b.start, h->sstream));
+  CK(h, launch_sampler(p, h->max_region, b.entry_prefix, h->sstream));
+  CK(h, cudaEventRecord(b.ready, h->sstream));
+  h->n_sampled++;
+  return FW2V_OK;
+}
+
+// The most recently sampled epoch's set, complete.
+static fw2v_status last_sampled(fw2v_handle* h, SampleBuf** out) {
+  if (!h || h->n_sampled == 0) return fail(h, FW2V_ERR_STATE, "no sampled epoch");
+  SampleBuf& b = h->buf[(h->n_sampled - 1) % 2];
+  CK(h, cudaEventSynchronize(b.ready));
+  *out = &b;
   return FW2V_OK;
 }
 
 fw2v_status fw2v_epoch_sample_sizes(fw2v_handle* h, int64_t* n_entries, int64_t* n_kept) {
-  if (!h || !h->sampled) return fail(h, FW2V_ERR_STATE, "no sampled epoch");
+  SampleBuf* b = nullptr;
+  fw2v_status st = last_sampled(h, &b);
+  if (st != FW2V_OK) return st;
   const int T = h->cfg.threads;
   std::vector<int64_t> ne(T), nk(T);
-  CK(h, cudaMemcpyAsync(ne.data(), h->n_entries, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
-  CK(h, cudaMemcpyAsync(nk.data(), h->n_kept, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
-  fw2v_status s = check_flag(h, "sample_epoch");
-  if (s != FW2V_OK) return s;
-  int64_t a = 0, b = 0;
+  CK(h, cudaMemcpyAsync(ne.data(), b->n_entries, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaMemcpyAsync(nk.data(), b->n_kept, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+  st = check_flag(h, "sample_epoch");
+  if (st != FW2V_OK) return st;
+  int64_t a = 0, c = 0;
   for (int i = 0; i < T; i++) {
     a += ne[i];
-    b += nk[i];
+    c += nk[i];
   }
   if (n_entries) *n_entries = a;
-  if (n_kept) *n_kept = b;
+  if (n_kept) *n_kept = c;
   return FW2V_OK;
 }
 
 fw2v_status fw2v_epoch_samples(fw2v_handle* h, int32_t* lens, float* alphas, int32_t* ids, int32_t* negs,
                                int64_t* entries_per_stream, int64_t* kept_per_stream, uint64_t* words_per_stream) {
-  if (!h || !h->sampled) return fail(h, FW2V_ERR_STATE, "no sampled epoch");
+  SampleBuf* b = nullptr;
+  fw2v_status st = last_sampled(h, &b);
+  if (st != FW2V_OK) return st;
   const int T = h->cfg.threads;
   const int K = h->cfg.negative;
   std::vector<int64_t> ne(T), nk(T);
   std::vector<uint64_t> wr(T);
   std::vector<int64_t> off(h->n_chunks);
-  CK(h, cudaMemcpyAsync(ne.data(), h->n_entries, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
-  CK(h, cudaMemcpyAsync(nk.data(), h->n_kept, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
-  CK(h, cudaMemcpyAsync(wr.data(), h->words, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaMemcpyAsync(ne.data(), b->n_entries, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaMemcpyAsync(nk.data(), b->n_kept, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaMemcpyAsync(wr.data(), b->words, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
   CK(h, cudaMemcpyAsync(off.data(), h->chunk_off, h->n_chunks * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
-  fw2v_status st = check_flag(h, "sample_epoch");
+  st = check_flag(h, "sample_epoch");
   if (st != FW2V_OK) return st;
   int64_t eo = 0, ko = 0;
   for (int s = 0; s < T; s++) {
@@ -441,11 +486,11 @@ fw2v_status fw2v_epoch_samples(fw2v_handle* h, int32_t* lens, float* alphas, int
     stream_range(h->n_chunks, T, s, &first, &end);
     const int64_t kb = off[first];
     const int64_t eb = kb + 2 * (int64_t)s;
-    if (lens) CK(h, cudaMemcpyAsync(lens + eo, h->ent_len + eb, ne[s] * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
-    if (alphas) CK(h, cudaMemcpyAsync(alphas + eo, h->ent_alpha + eb, ne[s] * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
-    if (ids) CK(h, cudaMemcpyAsync(ids + ko, h->kept_ids + kb, nk[s] * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    if (lens) CK(h, cudaMemcpyAsync(lens + eo, b->ent_len + eb, ne[s] * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    if (alphas) CK(h, cudaMemcpyAsync(alphas + eo, b->ent_alpha + eb, ne[s] * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    if (ids) CK(h, cudaMemcpyAsync(ids + ko, b->kept_ids + kb, nk[s] * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
     if (negs && K > 0)
-      CK(h, cudaMemcpyAsync(negs + ko * K, h->kept_negs + kb * K, nk[s] * K * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+      CK(h, cudaMemcpyAsync(negs + ko * K, b->kept_negs + kb * K, nk[s] * K * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
     if (entries_per_stream) entries_per_stream[s] = ne[s];
     if (kept_per_stream) kept_per_stream[s] = nk[s];
     if (words_per_stream) words_per_stream[s] = wr[s];
@@ -456,30 +501,43 @@ fw2v_status fw2v_epoch_samples(fw2v_handle* h, int32_t* lens, float* alphas, int
   return FW2V_OK;
 }
 
-fw2v_status fw2v_train_sampled(fw2v_handle* h, fw2v_epoch_stats* stats) {
-  if (!h || !h->sampled) return fail(h, FW2V_ERR_STATE, "train_sampled without a sampled epoch");
+// Launch the trainer on the oldest sampled epoch (asynchronous).
+static fw2v_status launch_epoch_train(fw2v_handle* h, SampleBuf** used) {
+  if (!h || h->n_trained >= h->n_sampled) return fail(h, FW2V_ERR_STATE, "train_sampled without a sampled epoch");
   CK(h, cudaSetDevice(h->cfg.device));
+  SampleBuf& b = h->buf[h->n_trained % 2];
   TrainParams p = base_train_params(h);
-  p.ids = h->kept_ids;
-  p.negs = h->kept_negs;
+  p.ids = b.kept_ids;
+  p.negs = b.kept_negs;
   p.source = kSourceEpoch;
-  p.entry_prefix = h->entry_prefix;
+  p.entry_prefix = b.entry_prefix;
   p.chunk_off = h->chunk_off;
   p.n_chunks = h->n_chunks;
   p.threads = h->cfg.threads;
-  p.ent_start = h->ent_start;
-  p.ent_len = h->ent_len;
-  p.ent_alpha = h->ent_alpha;
+  p.ent_start = b.ent_start;
+  p.ent_len = b.ent_len;
+  p.ent_alpha = b.ent_alpha;
+  CK(h, cudaStreamWaitEvent(h->stream, b.ready, 0));
+  CK(h, cudaEventRecord(h->ev[1], h->stream));
   CK(h, cudaMemsetAsync(h->work_counter, 0, sizeof(unsigned long long), h->stream));
   CK(h, launch_train(p, h->num_sms, h->stream));
   CK(h, cudaEventRecord(h->ev[2], h->stream));
+  CK(h, cudaEventRecord(b.freed, h->stream));
+  b.used = true;
+  h->n_trained++;
+  *used = &b;
+  return FW2V_OK;
+}
+
+// Wait for the trainer, then count the epoch's words and fill the stats.
+static fw2v_status finish_epoch_train(fw2v_handle* h, SampleBuf* b, fw2v_epoch_stats* stats) {
   const int T = h->cfg.threads;
   std::vector<uint64_t> wr(T);
   std::vector<int64_t> ne(T), nk(T);
-  CK(h, cudaMemcpyAsync(wr.data(), h->words, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaMemcpyAsync(wr.data(), b->words, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
   if (stats) {
-    CK(h, cudaMemcpyAsync(ne.data(), h->n_entries, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
-    CK(h, cudaMemcpyAsync(nk.data(), h->n_kept, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaMemcpyAsync(ne.data(), b->n_entries, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaMemcpyAsync(nk.data(), b->n_kept, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
   }
   fw2v_status s = check_flag(h, "train");
   if (s != FW2V_OK) return s;
@@ -487,7 +545,6 @@ fw2v_status fw2v_train_sampled(fw2v_handle* h, fw2v_epoch_stats* stats) {
   for (int i = 0; i < T; i++) words += wr[i];
   h->words_total += words;
   h->epochs_done++;
-  h->sampled = false;
   if (stats) {
     stats->words_read = words;
     stats->words_kept = 0;
@@ -496,16 +553,35 @@ fw2v_status fw2v_train_sampled(fw2v_handle* h, fw2v_epoch_stats* stats) {
       stats->words_kept += (uint64_t)nk[i];
       stats->sentences += (uint64_t)ne[i];
     }
-    CK(h, cudaEventElapsedTime(&stats->sampler_ms, h->ev[0], h->ev[1]));
+    CK(h, cudaEventElapsedTime(&stats->sampler_ms, b->start, b->ready));
     CK(h, cudaEventElapsedTime(&stats->train_ms, h->ev[1], h->ev[2]));
   }
   return FW2V_OK;
 }
 
-fw2v_status fw2v_train_epoch(fw2v_handle* h, fw2v_epoch_stats* stats) {
-  fw2v_status s = fw2v_sample_epoch(h);
+fw2v_status fw2v_train_sampled(fw2v_handle* h, fw2v_epoch_stats* stats) {
+  SampleBuf* b = nullptr;
+  fw2v_status s = launch_epoch_train(h, &b);
   if (s != FW2V_OK) return s;
-  return fw2v_train_sampled(h, stats);
+  return finish_epoch_train(h, b, stats);
+}
+
+// One epoch: sample it unless that is already done, launch its trainer, and
+// while it runs sample the next epoch on the sampler stream (if the configured
+// epochs go on) so that sampling overlaps training.
+fw2v_status fw2v_train_epoch(fw2v_handle* h, fw2v_epoch_stats* stats) {
+  if (!h) return FW2V_ERR_ARGUMENT;
+  fw2v_status s = FW2V_OK;
+  if (h->n_sampled == h->n_trained) s = fw2v_sample_epoch(h);
+  if (s != FW2V_OK) return s;
+  SampleBuf* b = nullptr;
+  s = launch_epoch_train(h, &b);
+  if (s != FW2V_OK) return s;
+  if (h->n_sampled < h->cfg.epochs && h->n_sampled == h->n_trained) {
+    s = fw2v_sample_epoch(h);
+    if (s != FW2V_OK) return s;
+  }
+  return finish_epoch_train(h, b, stats);
 }
 
 fw2v_status fw2v_train(fw2v_handle* h, uint64_t* words_read) {
