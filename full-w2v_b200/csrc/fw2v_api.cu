@@ -199,6 +199,7 @@ const char* fw2v_status_string(fw2v_status s) {
     case FW2V_ERR_STATE: return "call out of order";
     case FW2V_ERR_BOUNDS: return "id out of range";
     case FW2V_ERR_NO_DEVICE: return "no usable CUDA device";
+    case FW2V_ERR_TOO_LARGE: return "request exceeds a fixed-size library buffer";
   }
   return "unknown status";
 }

@@ -97,6 +97,24 @@ extern "C" fw2v_status fw2v_kernel_batch(float* syn0, float* syn1neg, const int3
   return e == cudaSuccess ? FW2V_OK : FW2V_ERR_CUDA;
 }
 
+namespace fw2v {
+
+// The seam's per-device state (sigmoid table, sticky error word, SM count),
+// set up on first use; shared with the allocation-free variant of the seam.
+fw2v_status seam_state(int dev, int** error_word, const float** exp_table, int* sms) {
+  fw2v_status s = seam_setup(dev);
+  if (s != FW2V_OK) return s;
+  void* addr = nullptr;
+  if (cudaGetSymbolAddress(&addr, g_seam_error) != cudaSuccess) return FW2V_ERR_CUDA;
+  *error_word = (int*)addr;
+  if (cudaGetSymbolAddress(&addr, g_seam_exp_table) != cudaSuccess) return FW2V_ERR_CUDA;
+  *exp_table = (const float*)addr;
+  *sms = g_seam_sms[dev];
+  return FW2V_OK;
+}
+
+}  // namespace fw2v
+
 extern "C" fw2v_status fw2v_kernel_batch_error(void* stream) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return FW2V_ERR_NO_DEVICE;

@@ -22,7 +22,9 @@ LIB_PATH = os.path.join(os.path.dirname(HERE), "libfw2v.so")
 FP32, BF16 = 0, 1
 SIGMOID_TABLE, SIGMOID_EXACT = 0, 1
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory",
-          4: "call out of order", 5: "id out of range", 6: "no usable CUDA device"}
+          4: "call out of order", 5: "id out of range", 6: "no usable CUDA device",
+          7: "request exceeds a fixed-size library buffer"}
+NOALLOC_SCRATCH_BYTES = 16 << 20
 
 
 class Fw2vError(RuntimeError):
@@ -53,6 +55,7 @@ EXPORTS = [
     "fw2v_set_tables", "fw2v_train_sentences", "fw2v_heldout_loss", "fw2v_kernel_batch",
     "fw2v_kernel_batch_error", "fw2v_lane_layout", "fw2v_exp_table", "fw2v_unigram_firsts",
     "fw2v_get_unigram", "fw2v_status_string", "fw2v_last_error", "fw2v_version", "fw2v_stream",
+    "fw2v_kernel_batch_noalloc",
 ]
 
 _lib = None
@@ -89,6 +92,8 @@ def lib() -> C.CDLL:
             "fw2v_kernel_batch": (C.c_int, [P, P, P, P, P, P, I32, I32, I32, I32, I32,
                                             C.c_uint32, I64, P]),
             "fw2v_kernel_batch_error": (C.c_int, [P]),
+            "fw2v_kernel_batch_noalloc": (C.c_int, [P, P, P, P, P, P, I32, I32, I32, I32, I32,
+                                                    C.c_uint32, I64, P]),
             "fw2v_lane_layout": (None, [I32, I32, C.POINTER(I32), C.POINTER(I32),
                                         C.POINTER(I64)]),
             "fw2v_exp_table": (None, [P]),

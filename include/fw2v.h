@@ -52,7 +52,8 @@ typedef enum fw2v_status {
   FW2V_ERR_NOMEM = 3,        /* device or pinned host allocation failed */
   FW2V_ERR_STATE = 4,        /* call out of order (e.g. train before set_vocab) */
   FW2V_ERR_BOUNDS = 5,       /* a token or negative id outside [0, V) was found */
-  FW2V_ERR_NO_DEVICE = 6     /* no CUDA device or the library was built for another arch */
+  FW2V_ERR_NO_DEVICE = 6,    /* no CUDA device or the library was built for another arch */
+  FW2V_ERR_TOO_LARGE = 7     /* the request does not fit a fixed-size library buffer */
 } fw2v_status;
 
 typedef enum fw2v_sigmoid {
@@ -160,6 +161,35 @@ fw2v_status fw2v_kernel_batch(float* syn0, float* syn1neg, const int32_t* sen, c
                               const int32_t* len, const float* alpha, int32_t n_blocks,
                               int32_t layer_size, int32_t window, int32_t negative, int32_t msl,
                               uint32_t pitch, int64_t vocab_size, void* stream);
+/* fw2v_kernel_batch without any device allocation.  No counterpart in the
+ * reference: FULL-W2V allocates all of its buffers up front in its driver.
+ *
+ * For callers that must not allocate device memory: code that runs while a
+ * stream is being captured into a CUDA graph (cudaMalloc/cudaFree cannot be
+ * captured and cudaFree synchronises the device), programs whose device memory
+ * is owned entirely by a framework's pooling allocator, and latency-bound loops
+ * that cannot absorb an allocator call.  Arguments and results are those of
+ * fw2v_kernel_batch.  The per-warp scratch the kernel needs (each context row's
+ * value when it entered the window) lives in a fixed array of
+ * FW2V_NOALLOC_SCRATCH_BYTES inside the library, which every GPU that loads the
+ * library keeps until the process exits; (2*window+1) * pitch * 4 bytes per warp
+ * of up to FW2V_NOALLOC_SCRATCH_BYTES in total cap the number of warps working
+ * concurrently.  A request needing more than that for one block of 4 warps is
+ * rejected with FW2V_ERR_TOO_LARGE before anything runs.
+ *
+ * The first call on a device looks up the array's device address and loads the
+ * sigmoid table; make that first call before any stream capture.  All calls
+ * share the one array and nothing in it needs to start at zero (every row is
+ * written when it enters the window, before it is read), so its contents from
+ * an earlier call are harmless; but calls that overlap on the GPU (other
+ * streams, or another thread) race on it and must be serialised by the caller.
+ * Out-of-range ids are reported by fw2v_kernel_batch_error, like the seam's. */
+#define FW2V_NOALLOC_SCRATCH_BYTES (16u << 20)
+fw2v_status fw2v_kernel_batch_noalloc(float* syn0, float* syn1neg, const int32_t* sen,
+                                      const int32_t* neg, const int32_t* len, const float* alpha,
+                                      int32_t n_blocks, int32_t layer_size, int32_t window,
+                                      int32_t negative, int32_t msl, uint32_t pitch,
+                                      int64_t vocab_size, void* stream);
 /* Returns FW2V_ERR_BOUNDS (and clears it) if an earlier fw2v_kernel_batch launch
  * on this device skipped a block with an out-of-range id; synchronises `stream`. */
 fw2v_status fw2v_kernel_batch_error(void* stream);
