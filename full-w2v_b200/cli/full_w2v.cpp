@@ -1,0 +1,581 @@
+// full-w2v: drop-in command line for the FULL-W2V training program
+// (src/FULL-W2V/FULL-W2V-driver.cu + improved_driver_functions.cpp +
+// legacy_driver_functions.cpp), training on a B200 through libfw2v.
+//
+// Same flags and defaults (improved_driver_functions.cpp:403-501), same text
+// front end (word reader, vocabulary, global token stream, vocabulary and corpus
+// cache files), same .vec output (improved_driver_functions.cpp:225-242) and the
+// same closing lines "Overall Words Per Second / Overall Words / Overall time"
+// (FULL-W2V-driver.cu:450-451) that replication/sweep.py parses.
+//
+// Flags the GPU path has no use for (-streams, -kernel-batch-size) are accepted
+// and ignored.  Added flags: -sigmoid table|exact, -deterministic 0|1,
+// -device N.  Without -threads the number of sampling streams is chosen for the
+// GPU (one stream per 256 stored sentences, at least 1, at most 4096) instead of
+// the reference's CPU-thread default of 12.
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "fw2v.h"
+
+namespace {
+
+constexpr int kMaxString = 800;               // FULL-W2V-driver.cu:16
+constexpr int64_t kVocabHashSize = 30000000;  // FULL-W2V-driver.cu:60 (reduce threshold 0.7x)
+
+struct Options {
+  std::string train, output, save_vocab, read_vocab, save_corpus, save_corpus_cache, read_corpus_cache;
+  bool do_export = true, recount = false, cache_eos = false, pre_shuffle = false, epoch_shuffle = false;
+  int binary = 0, debug = 2, min_count = 5, layer_size = 100, epochs = 5, window = 5, negative = 5;
+  int threads = -1, msl = 1000, sigmoid = FW2V_SIGMOID_TABLE, deterministic = 0, device = 0;
+  float alpha = 0.025f, sample = 1e-3f;
+};
+
+// ---------------------------------------------------------------------------
+// Mapped files and the word reader
+// ---------------------------------------------------------------------------
+struct Mapped {
+  const char* data = nullptr;
+  uint64_t size = 0;
+  bool open(const std::string& path) {
+    int fd = ::open(path.c_str(), O_RDONLY);
+    if (fd < 0) return false;
+    struct stat st;
+    if (fstat(fd, &st) < 0) {
+      ::close(fd);
+      return false;
+    }
+    size = (uint64_t)st.st_size;
+    if (size > 0) {
+      void* p = mmap(nullptr, size, PROT_READ, MAP_PRIVATE, fd, 0);
+      if (p == MAP_FAILED) {
+        ::close(fd);
+        return false;
+      }
+      data = (const char*)p;
+    }
+    ::close(fd);
+    return true;
+  }
+  ~Mapped() {
+    if (data) munmap((void*)data, size);
+  }
+};
+
+// One word from a mapped file (improved_driver_functions.cpp:86-124): CR is
+// skipped, a newline alone reads as "</s>", blanks and tabs separate words,
+// words are cut at 799 bytes and the rest of an over-long word is skipped.
+void read_word(std::string& word, const char* m, uint64_t max, uint64_t* cur) {
+  word.clear();
+  char c = 0;
+  uint64_t pos = *cur;
+  while (pos < max) {
+    c = m[pos++];
+    if (c == 13) continue;
+    if (c == '\n') {
+      if (!word.empty()) {
+        pos--;
+        break;
+      }
+      word = "</s>";
+      *cur = pos;
+      return;
+    }
+    if (c == ' ' || c == '\t') {
+      if (!word.empty()) break;
+      continue;
+    }
+    word.push_back(c);
+    if ((int)word.size() >= kMaxString - 1) break;
+  }
+  if (pos == max || c == ' ' || c == '\t' || c == '\n') {
+    *cur = pos;
+    return;
+  }
+  while (pos < max && c != ' ' && c != '\t' && c != '\n') c = m[pos++];
+  *cur = pos - 1;
+}
+
+// ---------------------------------------------------------------------------
+// Vocabulary (legacy_driver_functions.cpp:26-124, improved_driver_functions.cpp:136-223)
+// ---------------------------------------------------------------------------
+struct Vocab {
+  std::vector<std::string> words;
+  std::vector<uint64_t> counts;
+  std::unordered_map<std::string, int> index;
+  int64_t min_reduce = 1;
+
+  int find(const std::string& w) const {
+    auto it = index.find(w);
+    return it == index.end() ? -1 : it->second;
+  }
+  int add(const std::string& w) {
+    words.push_back(w.substr(0, kMaxString - 1));
+    counts.push_back(0);
+    index[words.back()] = (int)words.size() - 1;
+    return (int)words.size() - 1;
+  }
+  void rebuild_index() {
+    index.clear();
+    for (size_t i = 0; i < words.size(); i++) index.emplace(words[i], (int)i);
+  }
+  // Drop words seen at most min_reduce times (ReduceVocab).
+  void reduce() {
+    size_t k = 0;
+    for (size_t i = 0; i < words.size(); i++) {
+      if (counts[i] > (uint64_t)min_reduce) {
+        words[k] = words[i];
+        counts[k] = counts[i];
+        k++;
+      }
+    }
+    words.resize(k);
+    counts.resize(k);
+    rebuild_index();
+    min_reduce++;
+  }
+  // Sort by count, "</s>" kept at 0, cut below min_count; returns the sum of the
+  // remaining counts (SortVocab).  Ties keep their order: the reference's qsort
+  // is glibc's stable merge sort.
+  uint64_t sort_and_cut(int min_count) {
+    std::vector<size_t> order(words.size());
+    for (size_t i = 0; i < order.size(); i++) order[i] = i;
+    if (order.size() > 1)
+      std::stable_sort(order.begin() + 1, order.end(),
+                       [&](size_t a, size_t b) { return counts[a] > counts[b]; });
+    std::vector<std::string> w2;
+    std::vector<uint64_t> c2;
+    uint64_t total = 0;
+    for (size_t k = 0; k < order.size(); k++) {
+      size_t i = order[k];
+      if (counts[i] < (uint64_t)min_count && k != 0) continue;
+      w2.push_back(words[i]);
+      c2.push_back(counts[i]);
+      total += counts[i];
+    }
+    words.swap(w2);
+    counts.swap(c2);
+    rebuild_index();
+    return total;
+  }
+};
+
+// LearnVocabFromTrainFile (improved_driver_functions.cpp:136-164).  The word
+// that ends exactly at the end of the file is not counted.
+uint64_t learn_vocab(Vocab& v, const Mapped& f, int min_count) {
+  v.add("</s>");
+  std::string w;
+  uint64_t train_words = 0;
+  for (uint64_t pos = 0; pos < f.size;) {
+    read_word(w, f.data, f.size, &pos);
+    if (pos == f.size) break;
+    train_words++;
+    int i = v.find(w);
+    if (i < 0) {
+      i = v.add(w);
+      v.counts[i] = 1;
+    } else {
+      v.counts[i]++;
+    }
+    if ((int64_t)v.words.size() > (int64_t)(kVocabHashSize * 0.7)) v.reduce();
+  }
+  (void)train_words;
+  return v.sort_and_cut(min_count) + 1;
+}
+
+// ReadVocab (improved_driver_functions.cpp:167-196): "word count" per line.
+bool read_vocab(Vocab& v, const std::string& path, int min_count, uint64_t* train_words) {
+  Mapped f;
+  if (!f.open(path)) return false;
+  std::string w, c;
+  for (uint64_t pos = 0; pos < f.size; pos++) {
+    read_word(w, f.data, f.size, &pos);
+    int i = v.add(w);
+    read_word(c, f.data, f.size, &pos);
+    v.counts[i] = (uint64_t)(uint32_t)atoi(c.c_str());
+  }
+  *train_words = v.sort_and_cut(min_count);
+  return true;
+}
+
+// recountVocab (improved_driver_functions.cpp:199-223).
+uint64_t recount_vocab(Vocab& v, const Mapped& f, int min_count) {
+  std::fill(v.counts.begin(), v.counts.end(), 0);
+  std::string w;
+  for (uint64_t pos = 0; pos < f.size;) {
+    read_word(w, f.data, f.size, &pos);
+    int i = v.find(w);
+    if (i >= 0) v.counts[i]++;
+  }
+  return v.sort_and_cut(min_count);
+}
+
+bool save_vocab(const Vocab& v, const std::string& path) {
+  FILE* fo = fopen(path.c_str(), "wb");
+  if (!fo) return false;
+  for (size_t i = 0; i < v.words.size(); i++) fprintf(fo, "%s %d\n", v.words[i].c_str(), (int)v.counts[i]);
+  fclose(fo);
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Corpus: the global token stream cut into stored chunks
+// ---------------------------------------------------------------------------
+struct Corpus {
+  std::vector<int32_t> stream;     // trailing 0 included
+  std::vector<int64_t> chunk_off;  // start of each stored chunk
+};
+
+// createGlobalStream (improved_driver_functions.cpp:244-281): in-vocabulary
+// words only, "</s>" kept with -cache-eos, a chunk ends after msl words or at
+// "</s>".  A run of out-of-vocabulary words reaching the end of the file stores
+// nothing (the reference stores -1 there).
+void create_stream(Corpus& c, const Vocab& v, const Mapped& f, int msl, bool cache_eos) {
+  std::string w;
+  int64_t sent_length = 0;
+  for (uint64_t pos = 0; pos < f.size;) {
+    int id = -1;
+    while (pos < f.size && id == -1) {
+      read_word(w, f.data, f.size, &pos);
+      id = v.find(w);
+    }
+    if (id == -1) break;
+    if (!cache_eos && id == 0) continue;
+    if (sent_length == 0) c.chunk_off.push_back((int64_t)c.stream.size());
+    c.stream.push_back(id);
+    sent_length++;
+    if (id == 0 || sent_length >= msl) sent_length = 0;
+  }
+  c.stream.push_back(0);
+}
+
+// saveCorpusCache / saveCorpus (improved_driver_functions.cpp:293-318).
+bool save_corpus(const Corpus& c, const Vocab& v, uint64_t train_words, int msl, const std::string& path,
+                 bool as_words) {
+  FILE* fo = fopen(path.c_str(), "w");
+  if (!fo) return false;
+  if (!as_words) fprintf(fo, "%llu %llu\n", (unsigned long long)c.chunk_off.size(), (unsigned long long)train_words);
+  for (int64_t off : c.chunk_off) {
+    int w = 0;
+    for (; w < msl && c.stream[off + w] != 0; w++) {
+      if (as_words) fprintf(fo, "%s ", v.words[c.stream[off + w]].c_str());
+      else fprintf(fo, "%u ", (unsigned)c.stream[off + w]);
+    }
+    if (w > 0) fprintf(fo, "\n");
+  }
+  fclose(fo);
+  return true;
+}
+
+// readCorpusCache (improved_driver_functions.cpp:320-401): "S N" then ids; a
+// "</s>" ends a chunk (stored with -cache-eos), and every msl+1-th id starts a
+// new chunk after an inserted 0.
+bool read_corpus_cache(Corpus& c, const std::string& path, int msl, bool cache_eos, uint64_t* train_words) {
+  Mapped f;
+  if (!f.open(path)) return false;
+  std::string w;
+  uint64_t pos = 0;
+  read_word(w, f.data, f.size, &pos);
+  read_word(w, f.data, f.size, &pos);
+  *train_words = (uint64_t)atoi(w.c_str());
+  pos++;
+  c.chunk_off.push_back(0);
+  uint64_t msl_trigger = 0;
+  auto new_chunk = [&]() {
+    c.stream.push_back(0);
+    c.chunk_off.push_back((int64_t)c.stream.size());
+    msl_trigger = 0;
+  };
+  while (pos < f.size) {
+    read_word(w, f.data, f.size, &pos);
+    if (w == "</s>") {
+      if (cache_eos) new_chunk();
+    } else {
+      if (msl_trigger == (uint64_t)msl) new_chunk();
+      else msl_trigger++;
+      c.stream.push_back(atoi(w.c_str()));
+    }
+  }
+  // The last chunk pointer points past the data (the reference's count is
+  // sentence_pos - 1); drop it and close the stream.
+  c.chunk_off.pop_back();
+  c.stream.push_back(0);
+  return true;
+}
+
+// shuffleSentences (improved_driver_functions.cpp:283-291) with the C library's
+// rand(), unseeded as in the reference.
+void shuffle_chunks(std::vector<int64_t>& off) {
+  if (off.empty()) return;
+  for (uint64_t i = off.size() - 1; i > 0; i--) {
+    uint64_t j = (uint64_t)((rand() / (double)RAND_MAX) * (double)(i + 1));
+    if (j >= off.size()) j = off.size() - 1;  // rand() == RAND_MAX picks i+1
+    std::swap(off[j], off[i]);
+  }
+}
+
+// saveModel (improved_driver_functions.cpp:225-242).
+bool save_model(const std::string& path, const Vocab& v, const std::vector<float>& syn0, int d, int binary) {
+  FILE* fo = fopen(path.c_str(), "wb");
+  if (!fo) return false;
+  fprintf(fo, "%d %d\n", (int)v.words.size(), d);
+  for (size_t a = 0; a < v.words.size(); a++) {
+    fprintf(fo, "%s ", v.words[a].c_str());
+    const float* row = syn0.data() + a * d;
+    if (binary) fwrite(row, sizeof(float), d, fo);
+    else
+      for (int b = 0; b < d; b++) fprintf(fo, "%f ", row[b]);
+    fprintf(fo, "\n");
+  }
+  fclose(fo);
+  return true;
+}
+
+double now_s() {
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC_RAW, &t);
+  return (double)t.tv_sec + t.tv_nsec / 1e9;
+}
+
+int arg_pos(const char* name, int argc, char** argv) {
+  for (int a = 1; a < argc; a++)
+    if (!strcmp(name, argv[a])) return a;
+  return -1;
+}
+
+void usage(const char* prog) {
+  printf("SGNS word2vec (FULL-W2V method) trained on an NVIDIA B200\n\nOptions:\n");
+  printf("** FILES & I/O **\n");
+  printf("\t-train <file>\t\tUse text data from <file> to train the model\n");
+  printf("\t-output <file>\t\tUse <file> to save the resulting word vectors\n");
+  printf("\t-no-export\t\tSkip exporting vectors after training\n");
+  printf("\t-binary <int>\t\tSave the vectors in binary mode; default is 0 (off)\n");
+  printf("\t-debug <int>\t\tDebug mode (default 2)\n");
+  printf("\t-save-vocab <file>\tSave the vocabulary to <file>\n");
+  printf("\t-read-vocab <file>\tRead the vocabulary from <file>\n");
+  printf("\t-min-count <int>\tDiscard words that appear less than <int> times; default 5\n");
+  printf("\t-recount\t\tRecount vocabulary counts from the training data\n");
+  printf("\t-save-corpus <file>\tSave the corpus as interpreted\n");
+  printf("\t-save-corpus-cache <file>\tSave the corpus cache\n");
+  printf("\t-read-corpus-cache <file>\tRead the corpus cache instead of the training data\n");
+  printf("\t-cache-eos\t\tKeep line ends as sentence ends\n");
+  printf("\t-pre-shuffle\t\tShuffle sentences before the first epoch\n");
+  printf("\t-epoch-shuffle\t\tShuffle sentences after each epoch\n");
+  printf("** TRAINING PARAMETERS **\n");
+  printf("\t-size <int>\t\tSize of word vectors; default 100\n");
+  printf("\t-epoch(s), -iter(s) <int>\tNumber of epochs; default 5\n");
+  printf("\t-alpha <float>\t\tStarting learning rate; default 0.025\n");
+  printf("\t-window <int>\t\tMax skip length; default 5 (1..15)\n");
+  printf("\t-sample <float>\t\tSubsampling threshold; default 1e-3\n");
+  printf("\t-negative(s) <int>\tNegative examples; default 5 (0..31)\n");
+  printf("\t-sigmoid table|exact\tSigmoid: the reference's 1000-entry table (default) or exact\n");
+  printf("\t-deterministic 0|1\tTrain sentences one at a time in stream order\n");
+  printf("** PARALLEL UTILIZATION **\n");
+  printf("\t-thread(s) <int>\tSampling streams (the reference's CPU threads); default: one per 256 sentences\n");
+  printf("\t-max-sentence-length, -msl <int>\tMaximum sentence length; default 1000\n");
+  printf("\t-device <int>\t\tCUDA device; default 0\n");
+  printf("\t-streams, -kernel-batch-size <int>\tAccepted for compatibility, unused\n");
+  printf("\nExamples:\n%s -train data.txt -output vec.txt -size 128 -window 5 -sample 1e-4 -negative 5 -epoch 3\n\n",
+         prog);
+}
+
+bool parse(int argc, char** argv, Options& o) {
+  if (argc == 1 || arg_pos("-help", argc, argv) > 0) {
+    usage(argv[0]);
+    return false;
+  }
+  auto val = [&](const char* n) -> const char* {
+    int i = arg_pos(n, argc, argv);
+    return (i > 0 && i + 1 < argc) ? argv[i + 1] : nullptr;
+  };
+  auto first = [&](std::initializer_list<const char*> ns) -> const char* {
+    for (const char* n : ns)
+      if (const char* v = val(n)) return v;
+    return nullptr;
+  };
+  if (const char* v = val("-output")) o.output = v;
+  if (arg_pos("-no-export", argc, argv) > 0) o.do_export = false;
+  if (const char* v = val("-binary")) o.binary = atoi(v);
+  if (const char* v = val("-debug")) o.debug = atoi(v);
+  if (const char* v = val("-save-vocab")) o.save_vocab = v;
+  if (const char* v = val("-read-vocab")) o.read_vocab = v;
+  if (const char* v = val("-train")) o.train = v;
+  if (const char* v = val("-min-count")) o.min_count = atoi(v);
+  if (arg_pos("-recount", argc, argv) > 0) o.recount = true;
+  if (const char* v = val("-save-corpus")) o.save_corpus = v;
+  if (const char* v = val("-save-corpus-cache")) o.save_corpus_cache = v;
+  if (const char* v = val("-read-corpus-cache")) o.read_corpus_cache = v;
+  if (arg_pos("-cache-eos", argc, argv) > 0) o.cache_eos = true;
+  if (arg_pos("-pre-shuffle", argc, argv) > 0) o.pre_shuffle = true;
+  if (arg_pos("-epoch-shuffle", argc, argv) > 0) o.epoch_shuffle = true;
+  if (const char* v = val("-size")) o.layer_size = atoi(v);
+  if (const char* v = first({"-epoch", "-epochs", "-iter", "-iters"})) o.epochs = atoi(v);
+  if (const char* v = val("-alpha")) o.alpha = (float)atof(v);
+  if (const char* v = val("-window")) o.window = atoi(v);
+  if (const char* v = val("-sample")) o.sample = (float)atof(v);
+  if (const char* v = first({"-negative", "-negatives"})) o.negative = atoi(v);
+  if (const char* v = first({"-thread", "-threads"})) o.threads = atoi(v);
+  if (const char* v = first({"-msl", "-max-sentence-length"})) o.msl = atoi(v);
+  if (const char* v = val("-sigmoid")) o.sigmoid = !strcmp(v, "exact") ? FW2V_SIGMOID_EXACT : FW2V_SIGMOID_TABLE;
+  if (const char* v = val("-deterministic")) o.deterministic = atoi(v);
+  if (const char* v = val("-device")) o.device = atoi(v);
+  return true;
+}
+
+int fail_status(const char* what, fw2v_status s, fw2v_handle* h) {
+  fprintf(stderr, "ERROR: %s: %s%s%s\n", what, fw2v_status_string(s), h ? ": " : "", h ? fw2v_last_error(h) : "");
+  return 1;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  Options o;
+  if (!parse(argc, argv, o)) return 0;
+  if (o.debug > 0) {
+    fprintf(stderr, "** FILES & I/O **\n");
+    if (!o.do_export && !o.output.empty()) fprintf(stderr, "!!\tProcess will train but will not export a model!\n");
+    else if (!o.output.empty()) fprintf(stderr, "Trained model will export to file: %s\n", o.output.c_str());
+    else fprintf(stderr, "!!\tPreprocessing only -- no training.\n");
+    fprintf(stderr, "layer size: %d, epochs: %d, alpha: %.5f, window: %d, sample: %f, negative: %d\n",
+            o.layer_size, o.epochs, o.alpha, o.window, o.sample, o.negative);
+  }
+
+  // SetupNetwork (FULL-W2V-driver.cu:356-425)
+  Vocab vocab;
+  Corpus corpus;
+  uint64_t train_words = 0;
+  if (!o.train.empty()) {
+    Mapped f;
+    if (!f.open(o.train)) {
+      printf("ERROR: Training data not found!\n");
+      return 1;
+    }
+    if (o.debug > 0) printf("Train file size = %lluK\n", (unsigned long long)(f.size / 1000));
+    if (!o.read_vocab.empty()) {
+      if (!read_vocab(vocab, o.read_vocab, o.min_count, &train_words)) {
+        printf("Vocabulary file \"%s\" not found!\n", o.read_vocab.c_str());
+        return 1;
+      }
+    } else {
+      train_words = learn_vocab(vocab, f, o.min_count);
+    }
+    if (o.recount) train_words = recount_vocab(vocab, f, o.min_count);
+    if (!o.save_vocab.empty()) save_vocab(vocab, o.save_vocab);
+    if (!o.read_corpus_cache.empty()) {
+      if (!read_corpus_cache(corpus, o.read_corpus_cache, o.msl, o.cache_eos, &train_words)) {
+        printf("Corpus cache file \"%s\" not found!\n", o.read_corpus_cache.c_str());
+        return 1;
+      }
+    } else {
+      create_stream(corpus, vocab, f, o.msl, o.cache_eos);
+    }
+  } else {
+    if (o.read_vocab.empty()) {
+      printf("ERROR: No vocabulary or training file to generate vocabulary from! Please specify -train or -read-vocab\n");
+      return 1;
+    }
+    if (!read_vocab(vocab, o.read_vocab, o.min_count, &train_words)) {
+      printf("Vocabulary file \"%s\" not found!\n", o.read_vocab.c_str());
+      return 1;
+    }
+    if (!o.save_vocab.empty()) save_vocab(vocab, o.save_vocab);
+    if (o.read_corpus_cache.empty()) {
+      printf("ERROR: No corpus cache or training file to learn from! Please specify -train or -read-corpus-cache\n");
+      return 1;
+    }
+    if (!read_corpus_cache(corpus, o.read_corpus_cache, o.msl, o.cache_eos, &train_words)) {
+      printf("Corpus cache file \"%s\" not found!\n", o.read_corpus_cache.c_str());
+      return 1;
+    }
+  }
+  if (!o.save_corpus_cache.empty()) save_corpus(corpus, vocab, train_words, o.msl, o.save_corpus_cache, false);
+  if (!o.save_corpus.empty()) save_corpus(corpus, vocab, train_words, o.msl, o.save_corpus, true);
+  const int64_t n_chunks = (int64_t)corpus.chunk_off.size();
+  if (o.threads < 0) o.threads = (int)std::max<int64_t>(1, std::min<int64_t>(4096, n_chunks / 256));
+  if (o.debug > 1)
+    printf("%lld sentences spread across %d sampling streams == %lld sentences/stream\n", (long long)n_chunks,
+           o.threads, (long long)(n_chunks / std::max(o.threads, 1)));
+  if (o.output.empty()) return 0;
+  if (n_chunks == 0) {
+    printf("ERROR: the corpus holds no in-vocabulary words\n");
+    return 1;
+  }
+  if (o.pre_shuffle) shuffle_chunks(corpus.chunk_off);
+
+  // InitNet + Train_SGNS through libfw2v
+  fw2v_config cfg;
+  fw2v_config_default(&cfg);
+  cfg.layer_size = o.layer_size;
+  cfg.window = o.window;
+  cfg.negative = o.negative;
+  cfg.epochs = o.epochs;
+  cfg.threads = o.threads;
+  cfg.msl = o.msl;
+  cfg.alpha = o.alpha;
+  cfg.sample = o.sample;
+  cfg.sigmoid = o.sigmoid;
+  cfg.deterministic = o.deterministic;
+  cfg.device = o.device;
+  fw2v_handle* h = nullptr;
+  fw2v_status st = fw2v_create(&cfg, &h);
+  if (st != FW2V_OK) return fail_status("create", st, nullptr);
+  std::vector<uint32_t> counts(vocab.counts.size());
+  for (size_t i = 0; i < counts.size(); i++) counts[i] = (uint32_t)vocab.counts[i];
+  if ((st = fw2v_set_vocab(h, counts.data(), (int64_t)counts.size(), train_words)) != FW2V_OK)
+    return fail_status("set_vocab", st, h);
+  if ((st = fw2v_load_corpus(h, corpus.stream.data(), (int64_t)corpus.stream.size(), corpus.chunk_off.data(),
+                             n_chunks)) != FW2V_OK)
+    return fail_status("load_corpus", st, h);
+
+  const double t0 = now_s();
+  uint64_t words = 0;
+  for (int e = 0; e < o.epochs; e++) {
+    fw2v_epoch_stats es;
+    if (o.epoch_shuffle) {
+      if ((st = fw2v_sample_epoch(h)) != FW2V_OK || (st = fw2v_train_sampled(h, &es)) != FW2V_OK)
+        return fail_status("train", st, h);
+      if (e + 1 < o.epochs) {
+        shuffle_chunks(corpus.chunk_off);
+        if ((st = fw2v_reorder_chunks(h, corpus.chunk_off.data(), n_chunks)) != FW2V_OK)
+          return fail_status("reorder_chunks", st, h);
+      }
+    } else if ((st = fw2v_train_epoch(h, &es)) != FW2V_OK) {
+      return fail_status("train", st, h);
+    }
+    words += es.words_read;
+    if (o.debug > 0) {
+      printf("%cEpoch %d/%d  Words: %llu  Words/sec: %.2fk", 13, e + 1, o.epochs, (unsigned long long)words,
+             words / 1000.0 / std::max(now_s() - t0, 1e-9));
+      fflush(stdout);
+    }
+  }
+  const double t1 = now_s();
+  printf("\nOverall Words Per Second: %.4f\n", words / (t1 - t0));
+  printf("Overall Words: %llu\nOverall time: %f\n", (unsigned long long)words, t1 - t0);
+
+  if (o.do_export) {
+    std::vector<float> syn0(counts.size() * (size_t)o.layer_size);
+    if ((st = fw2v_get_syn0(h, syn0.data(), o.layer_size)) != FW2V_OK) return fail_status("get_syn0", st, h);
+    if (o.debug > 0) fprintf(stderr, "Saving model to: %s\n", o.output.c_str());
+    if (!save_model(o.output, vocab, syn0, o.layer_size, o.binary)) {
+      fprintf(stderr, "ERROR: cannot write %s\n", o.output.c_str());
+      return 1;
+    }
+  }
+  fw2v_destroy(h);
+  return 0;
+}

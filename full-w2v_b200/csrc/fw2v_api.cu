@@ -25,6 +25,9 @@ cudaError_t launch_init_tables(float* syn0, int64_t V, int d, int64_t pitch, con
 size_t train_smem_bytes(int window, int64_t pitch, int warps, int r);
 int64_t train_scratch_warps(int num_sms);
 cudaError_t launch_validate_ids(const int32_t* ids, int64_t n, int64_t vocab, int* flag, cudaStream_t st);
+cudaError_t launch_corpus_layout(const int32_t* stream, int64_t stream_len, const int64_t* chunk_off,
+                                 int64_t n_chunks, int msl, int threads, int64_t* chunk_base,
+                                 int64_t* stream_base, cudaStream_t st);
 }  // namespace fw2v
 
 using namespace fw2v;
@@ -68,6 +71,10 @@ struct fw2v_handle {
   int64_t stream_len = 0;
   int64_t* chunk_off = nullptr;
   int64_t n_chunks = 0;
+  int64_t* chunk_base = nullptr;   // n_chunks + 1: prefix of readable chunk lengths
+  int64_t* stream_base = nullptr;  // threads + 1: kept-id base of each stream
+  std::vector<int64_t> h_stream_base;
+  int64_t sample_cap = 0;          // kept-id capacity of a sampler output set
   int64_t max_region = 0;
 
   uint64_t* lcg = nullptr;
@@ -276,7 +283,7 @@ void fw2v_destroy(fw2v_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   dfree(h->syn0); dfree(h->syn1neg); dfree(h->keep_thr); dfree(h->unigram); dfree(h->exp_table);
   dfree(h->jump_a); dfree(h->jump_c);
-  dfree(h->stream_ids); dfree(h->chunk_off);
+  dfree(h->stream_ids); dfree(h->chunk_off); dfree(h->chunk_base); dfree(h->stream_base);
   if (h->sstream) cudaStreamSynchronize(h->sstream);
   dfree(h->lcg); dfree(h->wca); dfree(h->alpha);
   for (SampleBuf& b : h->buf) {
@@ -324,70 +331,112 @@ fw2v_status fw2v_set_vocab(fw2v_handle* h, const uint32_t* counts, int64_t V, ui
   return FW2V_OK;
 }
 
+// Readable length of each chunk, the kept-id base of each stream, and sampler
+// output sets large enough for them (grown when needed).
+static fw2v_status layout_streams(fw2v_handle* h) {
+  const int T = h->cfg.threads;
+  const int K = h->cfg.negative;
+  CK(h, launch_corpus_layout(h->stream_ids, h->stream_len, h->chunk_off, h->n_chunks, h->cfg.msl, T,
+                             h->chunk_base, h->stream_base, h->stream));
+  h->h_stream_base.assign(T + 1, 0);
+  CK(h, cudaMemcpyAsync(h->h_stream_base.data(), h->stream_base, (T + 1) * sizeof(int64_t),
+                        cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  h->max_region = 0;
+  for (int s = 0; s < T; s++)
+    h->max_region = std::max(h->max_region, h->h_stream_base[s + 1] - h->h_stream_base[s]);
+  const int64_t cap = std::max<int64_t>(h->h_stream_base[T], 1);
+  if (cap > h->sample_cap) {
+    for (SampleBuf& b : h->buf) {
+      CK(h, dalloc(b.kept_ids, cap));
+      CK(h, dalloc(b.kept_state, cap));
+      CK(h, dalloc(b.kept_negs, (size_t)cap * std::max(K, 1)));
+      CK(h, dalloc(b.ent_start, cap + 2 * (int64_t)T));
+      CK(h, dalloc(b.ent_len, cap + 2 * (int64_t)T));
+      CK(h, dalloc(b.ent_alpha, cap + 2 * (int64_t)T));
+      b.used = false;
+    }
+    h->sample_cap = cap;
+  }
+  return FW2V_OK;
+}
+
+static fw2v_status check_chunks(fw2v_handle* h, const int64_t* chunk_off, int64_t n_chunks, int64_t stream_len) {
+  if (h->cfg.threads > n_chunks || h->cfg.threads > 65535)
+    return fail(h, FW2V_ERR_ARGUMENT, "threads (%d) > sentence chunks (%lld)", h->cfg.threads,
+                (long long)n_chunks);
+  for (int64_t i = 0; i < n_chunks; i++) {
+    if (chunk_off[i] < 0 || chunk_off[i] >= stream_len)
+      return fail(h, FW2V_ERR_ARGUMENT, "chunk %lld starts outside the stream", (long long)i);
+  }
+  return FW2V_OK;
+}
+
 fw2v_status fw2v_load_corpus(fw2v_handle* h, const int32_t* stream, int64_t stream_len, const int64_t* chunk_off,
                              int64_t n_chunks) {
   if (!h || !stream || !chunk_off || stream_len < 1 || n_chunks < 1)
     return fail(h, FW2V_ERR_ARGUMENT, "load_corpus: empty corpus");
   if (h->V == 0) return fail(h, FW2V_ERR_STATE, "load_corpus before set_vocab");
-  if (h->cfg.threads > n_chunks || h->cfg.threads > 65535)
-    return fail(h, FW2V_ERR_ARGUMENT, "load_corpus: threads (%d) > sentence chunks (%lld)", h->cfg.threads,
-                (long long)n_chunks);
   if (stream[stream_len - 1] != 0) return fail(h, FW2V_ERR_ARGUMENT, "load_corpus: stream must end with 0");
-  for (int64_t i = 0; i < n_chunks; i++) {
-    if (chunk_off[i] < 0 || chunk_off[i] >= stream_len || (i > 0 && chunk_off[i] < chunk_off[i - 1]))
-      return fail(h, FW2V_ERR_ARGUMENT, "load_corpus: chunk offset %lld invalid", (long long)i);
-  }
+  fw2v_status s = check_chunks(h, chunk_off, n_chunks, stream_len);
+  if (s != FW2V_OK) return s;
   CK(h, cudaSetDevice(h->cfg.device));
   const int T = h->cfg.threads;
-  const int K = h->cfg.negative;
   // Nothing may still read the previous corpus.
   CK(h, cudaStreamSynchronize(h->sstream));
   CK(h, cudaStreamSynchronize(h->stream));
-  if (stream_len != h->stream_len || n_chunks != h->n_chunks || !h->stream_ids) {
-    CK(h, dalloc(h->stream_ids, stream_len));
+  if (stream_len != h->stream_len || !h->stream_ids) CK(h, dalloc(h->stream_ids, stream_len));
+  if (n_chunks != h->n_chunks || !h->chunk_off) {
     CK(h, dalloc(h->chunk_off, n_chunks));
+    CK(h, dalloc(h->chunk_base, n_chunks + 1));
+  }
+  if (!h->stream_base) {
+    CK(h, dalloc(h->stream_base, T + 1));
+    CK(h, dalloc(h->lcg, T));
+    CK(h, dalloc(h->wca, T));
+    CK(h, dalloc(h->alpha, T));
     for (SampleBuf& b : h->buf) {
-      CK(h, dalloc(b.kept_ids, stream_len));
-      CK(h, dalloc(b.kept_state, stream_len));
-      CK(h, dalloc(b.kept_negs, (size_t)stream_len * std::max(K, 1)));
-      CK(h, dalloc(b.ent_start, stream_len + 2 * (int64_t)T));
-      CK(h, dalloc(b.ent_len, stream_len + 2 * (int64_t)T));
-      CK(h, dalloc(b.ent_alpha, stream_len + 2 * (int64_t)T));
       CK(h, dalloc(b.n_entries, T));
       CK(h, dalloc(b.n_kept, T));
       CK(h, dalloc(b.words, T));
       CK(h, dalloc(b.entry_prefix, T + 1));
-      b.used = false;
     }
-    CK(h, dalloc(h->lcg, T));
-    CK(h, dalloc(h->wca, T));
-    CK(h, dalloc(h->alpha, T));
   }
   h->stream_len = stream_len;
   h->n_chunks = n_chunks;
-  h->max_region = 0;
-  for (int s = 0; s < T; s++) {
-    int64_t first, end;
-    stream_range(n_chunks, T, s, &first, &end);
-    const int64_t region = (end < n_chunks ? chunk_off[end] : stream_len) - chunk_off[first];
-    h->max_region = std::max(h->max_region, region);
-  }
   CK(h, cudaMemcpyAsync(h->stream_ids, stream, stream_len * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaMemcpyAsync(h->chunk_off, chunk_off, n_chunks * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
   CK(h, launch_validate_ids(h->stream_ids, stream_len, h->V, h->error_flag, h->stream));
+  s = layout_streams(h);
+  if (s != FW2V_OK) return s;
   // Stream state (FULL-W2V-driver.cu:113-114): LCG seeded with the id, alpha0.
   std::vector<uint64_t> lcg(T), zero(T, 0);
   std::vector<float> alpha(T, h->cfg.alpha);
-  for (int s = 0; s < T; s++) lcg[s] = (uint64_t)s;
+  for (int i = 0; i < T; i++) lcg[i] = (uint64_t)i;
   CK(h, cudaMemcpyAsync(h->lcg, lcg.data(), T * sizeof(uint64_t), cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaMemcpyAsync(h->wca, zero.data(), T * sizeof(uint64_t), cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaMemcpyAsync(h->alpha, alpha.data(), T * sizeof(float), cudaMemcpyHostToDevice, h->stream));
-  fw2v_status s = check_flag(h, "load_corpus");
+  s = check_flag(h, "load_corpus");
   if (s != FW2V_OK) return s;
   h->n_sampled = h->n_trained = 0;
   h->epochs_done = 0;
   h->words_total = 0;
   return FW2V_OK;
+}
+
+fw2v_status fw2v_reorder_chunks(fw2v_handle* h, const int64_t* chunk_off, int64_t n_chunks) {
+  if (!h || !chunk_off) return FW2V_ERR_ARGUMENT;
+  if (!h->stream_ids) return fail(h, FW2V_ERR_STATE, "reorder_chunks before load_corpus");
+  if (n_chunks != h->n_chunks) return fail(h, FW2V_ERR_ARGUMENT, "reorder_chunks: chunk count changed");
+  if (h->n_sampled != h->n_trained)
+    return fail(h, FW2V_ERR_STATE, "reorder_chunks with a sampled epoch not yet trained");
+  fw2v_status s = check_chunks(h, chunk_off, n_chunks, h->stream_len);
+  if (s != FW2V_OK) return s;
+  CK(h, cudaSetDevice(h->cfg.device));
+  CK(h, cudaStreamSynchronize(h->sstream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  CK(h, cudaMemcpyAsync(h->chunk_off, chunk_off, n_chunks * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
+  return layout_streams(h);
 }
 
 fw2v_status fw2v_sample_epoch(fw2v_handle* h) {
@@ -401,6 +450,7 @@ fw2v_status fw2v_sample_epoch(fw2v_handle* h) {
   p.stream_len = h->stream_len;
   p.chunk_off = h->chunk_off;
   p.n_chunks = h->n_chunks;
+  p.stream_base = h->stream_base;
   p.vocab = h->V;
   p.keep_thr = h->keep_thr;
   p.sample = h->cfg.sample;
@@ -474,18 +524,14 @@ fw2v_status fw2v_epoch_samples(fw2v_handle* h, int32_t* lens, float* alphas, int
   const int K = h->cfg.negative;
   std::vector<int64_t> ne(T), nk(T);
   std::vector<uint64_t> wr(T);
-  std::vector<int64_t> off(h->n_chunks);
   CK(h, cudaMemcpyAsync(ne.data(), b->n_entries, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
   CK(h, cudaMemcpyAsync(nk.data(), b->n_kept, T * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
   CK(h, cudaMemcpyAsync(wr.data(), b->words, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
-  CK(h, cudaMemcpyAsync(off.data(), h->chunk_off, h->n_chunks * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
   st = check_flag(h, "sample_epoch");
   if (st != FW2V_OK) return st;
   int64_t eo = 0, ko = 0;
   for (int s = 0; s < T; s++) {
-    int64_t first, end;
-    stream_range(h->n_chunks, T, s, &first, &end);
-    const int64_t kb = off[first];
+    const int64_t kb = h->h_stream_base[s];
     const int64_t eb = kb + 2 * (int64_t)s;
     if (lens) CK(h, cudaMemcpyAsync(lens + eo, b->ent_len + eb, ne[s] * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
     if (alphas) CK(h, cudaMemcpyAsync(alphas + eo, b->ent_alpha + eb, ne[s] * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
@@ -512,8 +558,7 @@ static fw2v_status launch_epoch_train(fw2v_handle* h, SampleBuf** used) {
   p.negs = b.kept_negs;
   p.source = kSourceEpoch;
   p.entry_prefix = b.entry_prefix;
-  p.chunk_off = h->chunk_off;
-  p.n_chunks = h->n_chunks;
+  p.stream_base = h->stream_base;
   p.threads = h->cfg.threads;
   p.ent_start = b.ent_start;
   p.ent_len = b.ent_len;

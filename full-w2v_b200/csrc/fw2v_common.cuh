@@ -59,6 +59,7 @@ struct SamplerParams {
   int64_t stream_len;
   const int64_t* chunk_off;
   int64_t n_chunks;
+  const int64_t* stream_base;  // threads + 1: where each stream's kept ids start
   int64_t vocab;
   const int32_t* keep_thr;  // keep a token iff (lcg & 0xFFFF) <= keep_thr[word]
   float sample;
@@ -114,8 +115,7 @@ struct TrainParams {
   int source;
   // kSourceEpoch
   const int64_t* entry_prefix;  // threads + 1
-  const int64_t* chunk_off;
-  int64_t n_chunks;
+  const int64_t* stream_base;   // threads + 1
   int threads;
   const int64_t* ent_start;
   const int32_t* ent_len;
@@ -137,11 +137,11 @@ struct TrainParams {
   int64_t scratch_warps;
 };
 
-__host__ __device__ __forceinline__ int64_t entry_base(const int64_t* chunk_off, int64_t n_chunks,
-                                                       int threads, int s) {
-  int64_t first, end;
-  stream_range(n_chunks, threads, s, &first, &end);
-  return chunk_off[first] + 2 * (int64_t)s;
+// Sampler output layout: stream s keeps its kept ids at [stream_base[s],
+// stream_base[s+1]) and its batch entries from stream_base[s] + 2s (one more
+// entry than kept ids at most, plus the epoch-end entry).
+__host__ __device__ __forceinline__ int64_t entry_base(const int64_t* stream_base, int s) {
+  return stream_base[s] + 2 * (int64_t)s;
 }
 
 }  // namespace fw2v

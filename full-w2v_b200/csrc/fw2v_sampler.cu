@@ -15,8 +15,9 @@
 // A second, fully parallel kernel turns each kept token's state into its K
 // negative ids (FULL-W2V-driver.cu:224-227).
 //
-// Output of one epoch, per stream s (kept_base(s) = chunk_off[first chunk],
-// entry_base(s) = kept_base(s) + 2s):
+// Output of one epoch, per stream s (kept_base(s) = stream_base[s], the sum of
+// the readable lengths of the chunks before the stream's range in chunk-table
+// order; entry_base(s) = kept_base(s) + 2s):
 //   entries  ent_{start,len,alpha}[entry_base(s) + e], e < n_entries[s]: every
 //            batch entry the reference records, zero-length ones included
 //   kept     kept_ids / kept_state[kept_base(s) + k], k < n_kept[s], and
@@ -39,10 +40,9 @@ __global__ void __launch_bounds__(128) sampler_warp_kernel(SamplerParams p) {
   if (s >= p.threads) return;
   int64_t es, ee;
   stream_range(p.n_chunks, p.threads, s, &es, &ee);
-  const int64_t kept_base = p.chunk_off[es];
-  const int64_t region_end = ee < p.n_chunks ? p.chunk_off[ee] : p.stream_len;
-  const int64_t kept_cap = region_end - kept_base;
-  const int64_t entry_b = kept_base + 2 * (int64_t)s;
+  const int64_t kept_base = p.stream_base[s];
+  const int64_t kept_cap = p.stream_base[s + 1] - kept_base;
+  const int64_t entry_b = entry_base(p.stream_base, s);
   const int64_t entry_cap = kept_cap + 2;
   const int K = p.negative;
   const int msl = p.msl;
@@ -181,9 +181,7 @@ __global__ void __launch_bounds__(256) negatives_kernel(SamplerParams p) {
   const int s = blockIdx.y;
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= p.threads || k >= p.n_kept[s]) return;
-  int64_t es, ee;
-  stream_range(p.n_chunks, p.threads, s, &es, &ee);
-  const int64_t slot = p.chunk_off[es] + k;
+  const int64_t slot = p.stream_base[s] + k;
   uint64_t r = p.kept_state[slot];
   int32_t* out = p.kept_negs + slot * p.negative;
   for (int j = 0; j < p.negative; j++) {
@@ -216,6 +214,82 @@ __global__ void __launch_bounds__(1024) entry_prefix_kernel(const int64_t* n_ent
     run += n_entries[i];
   }
   if (t == 1023) prefix[threads] = partial[1023];
+}
+
+// Readable length of every stored chunk: its tokens up to msl or up to and
+// including its first 0 (the reader stops there, FULL-W2V-driver.cu:196-212),
+// clipped at the end of the stream.  One warp per chunk.
+__global__ void __launch_bounds__(256) chunk_length_kernel(const int32_t* stream, int64_t stream_len,
+                                                           const int64_t* chunk_off, int64_t n_chunks, int msl,
+                                                           int64_t* len) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (c >= n_chunks) return;
+  const int64_t off = chunk_off[c];
+  int n = msl;
+  for (int cur0 = 0; cur0 < msl; cur0 += 32) {
+    const int cur = cur0 + lane;
+    const int64_t pos = off + cur;
+    const bool inb = cur < msl && pos < stream_len;
+    const unsigned end = __ballot_sync(kFull, !inb || stream[pos] == 0);
+    if (end) {
+      const int z = __ffs(end) - 1;  // first lane out of the stream or holding a 0
+      const int64_t zpos = off + cur0 + z;
+      n = cur0 + z + (zpos < stream_len ? 1 : 0);
+      if (n > msl) n = msl;
+      break;
+    }
+  }
+  if (lane == 0) len[c] = n;
+}
+
+// In-place exclusive prefix sum of n int64 values followed by their total at
+// index n (one block; the vectors here are chunk or stream counts).
+__global__ void __launch_bounds__(1024) exclusive_scan_kernel(int64_t* v, int64_t n) {
+  __shared__ int64_t partial[1024];
+  const int t = threadIdx.x;
+  const int64_t per = (n + 1023) / 1024;
+  const int64_t lo = t * per;
+  int64_t sum = 0;
+  for (int64_t i = lo; i < lo + per && i < n; i++) sum += v[i];
+  partial[t] = sum;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {
+    const int64_t x = t >= off ? partial[t - off] : 0;
+    __syncthreads();
+    partial[t] += x;
+    __syncthreads();
+  }
+  int64_t run = t > 0 ? partial[t - 1] : 0;
+  for (int64_t i = lo; i < lo + per && i < n; i++) {
+    const int64_t x = v[i];
+    v[i] = run;
+    run += x;
+  }
+  if (t == 1023) v[n] = partial[1023];
+}
+
+// stream_base[s] = chunk_base[first chunk of s]; stream_base[T] = total.
+__global__ void stream_base_kernel(const int64_t* chunk_base, int64_t n_chunks, int threads, int64_t* stream_base) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s > threads) return;
+  if (s == threads) {
+    stream_base[s] = chunk_base[n_chunks];
+    return;
+  }
+  int64_t first, end;
+  stream_range(n_chunks, threads, s, &first, &end);
+  stream_base[s] = chunk_base[first];
+}
+
+cudaError_t launch_corpus_layout(const int32_t* stream, int64_t stream_len, const int64_t* chunk_off,
+                                 int64_t n_chunks, int msl, int threads, int64_t* chunk_base,
+                                 int64_t* stream_base, cudaStream_t st) {
+  chunk_length_kernel<<<(unsigned)((n_chunks * 32 + 255) / 256), 256, 0, st>>>(stream, stream_len, chunk_off,
+                                                                             n_chunks, msl, chunk_base);
+  exclusive_scan_kernel<<<1, 1024, 0, st>>>(chunk_base, n_chunks);
+  stream_base_kernel<<<(threads + 1 + 255) / 256, 256, 0, st>>>(chunk_base, n_chunks, threads, stream_base);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_sampler(const SamplerParams& p, int64_t max_region, int64_t* entry_prefix,

@@ -297,7 +297,7 @@ __device__ __forceinline__ Sentence fetch_sentence(const TrainParams& p, int64_t
       if (p.entry_prefix[mid] <= w) lo = mid;
       else hi = mid - 1;
     }
-    const int64_t slot = entry_base(p.chunk_off, p.n_chunks, p.threads, lo) + (w - p.entry_prefix[lo]);
+    const int64_t slot = entry_base(p.stream_base, lo) + (w - p.entry_prefix[lo]);
     s.start = p.ent_start[slot];
     s.len = p.ent_len[slot];
     s.alpha = p.ent_alpha[slot];

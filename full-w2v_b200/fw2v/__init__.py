@@ -55,7 +55,7 @@ EXPORTS = [
     "fw2v_set_tables", "fw2v_train_sentences", "fw2v_heldout_loss", "fw2v_kernel_batch",
     "fw2v_kernel_batch_error", "fw2v_lane_layout", "fw2v_exp_table", "fw2v_unigram_firsts",
     "fw2v_get_unigram", "fw2v_status_string", "fw2v_last_error", "fw2v_version", "fw2v_stream",
-    "fw2v_kernel_batch_noalloc",
+    "fw2v_kernel_batch_noalloc", "fw2v_reorder_chunks",
 ]
 
 _lib = None
@@ -76,6 +76,7 @@ def lib() -> C.CDLL:
             "fw2v_destroy": (None, [H]),
             "fw2v_set_vocab": (C.c_int, [H, P, I64, U64]),
             "fw2v_load_corpus": (C.c_int, [H, P, I64, P, I64]),
+            "fw2v_reorder_chunks": (C.c_int, [H, P, I64]),
             "fw2v_sample_epoch": (C.c_int, [H]),
             "fw2v_epoch_sample_sizes": (C.c_int, [H, C.POINTER(I64), C.POINTER(I64)]),
             "fw2v_epoch_samples": (C.c_int, [H, P, P, P, P, P, P, P]),
@@ -192,6 +193,11 @@ class Trainer:
         chunk_off = np.ascontiguousarray(chunk_off, np.int64)
         self._check(lib().fw2v_load_corpus(self._h, _p(stream), len(stream), _p(chunk_off),
                                            len(chunk_off)), "load_corpus")
+
+    def reorder_chunks(self, chunk_off: np.ndarray):
+        chunk_off = np.ascontiguousarray(chunk_off, np.int64)
+        self._check(lib().fw2v_reorder_chunks(self._h, _p(chunk_off), len(chunk_off)),
+                    "reorder_chunks")
 
     # -- epoch loop ----------------------------------------------------------
     def sample_epoch(self):

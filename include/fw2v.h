@@ -105,9 +105,19 @@ fw2v_status fw2v_set_vocab(fw2v_handle* h, const uint32_t* counts, int64_t vocab
                            uint64_t train_words);
 
 /* Token stream (host memory; ids in [0, V), the trailing 0 included) and the
- * start offset of each stored sentence chunk.  Requires threads <= n_chunks. */
+ * start offset of each stored sentence chunk, in the order the streams read
+ * them (any order; a chunk is read from its offset up to msl tokens or up to
+ * and including its first 0).  Requires threads <= n_chunks.  Resets the
+ * streams' LCG and learning-rate state and the epoch count. */
 fw2v_status fw2v_load_corpus(fw2v_handle* h, const int32_t* stream, int64_t stream_len,
                              const int64_t* chunk_off, int64_t n_chunks);
+
+/* Replace the order of the stored chunks without touching the streams' LCG and
+ * learning-rate state: the reference's -epoch-shuffle, which permutes its
+ * sentence pointers between epochs (FULL-W2V-driver.cu:249-266,
+ * improved_driver_functions.cpp:283-291).  Same chunk count; call between
+ * epochs (no sampled epoch waiting to be trained). */
+fw2v_status fw2v_reorder_chunks(fw2v_handle* h, const int64_t* chunk_off, int64_t n_chunks);
 
 /* Run the on-device batch builder for the next epoch only. */
 fw2v_status fw2v_sample_epoch(fw2v_handle* h);

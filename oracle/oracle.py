@@ -356,6 +356,62 @@ def create_stream(buf: bytes, words, msl: int, cache_eos: bool):
     return np.array(stream, np.int32), np.array(chunk_off, np.int64)
 
 
+def _sort_cut(words, counts, min_count):
+    order = sorted(range(1, len(words)), key=lambda k: -counts[k])
+    order = [0] + [k for k in order if counts[k] >= min_count]
+    return [words[k] for k in order], [counts[k] for k in order]
+
+
+def read_vocab(buf: bytes, min_count: int):
+    """ReadVocab (improved_driver_functions.cpp:167-196): "word count" pairs,
+    then SortVocab.  train_words is the sum of the kept counts."""
+    words, counts = [], []
+    pos, n = 0, len(buf)
+    while pos < n:
+        w, pos = read_word(buf, pos)
+        c, pos = read_word(buf, pos)
+        words.append(w)
+        counts.append(int(c) & 0xFFFFFFFF if c.lstrip(b"-").isdigit() else 0)
+        pos += 1
+    words, counts = _sort_cut(words, counts, min_count)
+    return words, np.array(counts, np.uint32), int(sum(counts))
+
+
+def read_corpus_cache(buf: bytes, msl: int, cache_eos: bool):
+    """readCorpusCache (improved_driver_functions.cpp:320-401).
+
+    Header "S N": N is train_words.  A "</s>" ends a chunk when cache_eos; an
+    id arriving after msl ids of a chunk starts a new one (a 0 is stored between).
+    The last chunk pointer, which points past the last chunk started, is not a
+    sentence (sentence_count = pointers - 1), so that chunk is never read.
+    Returns (stream with a trailing 0, chunk offsets, train_words)."""
+    pos = 0
+    _, pos = read_word(buf, pos)
+    tw, pos = read_word(buf, pos)
+    pos += 1
+    stream, offs = [], [0]
+    trigger = 0
+    n = len(buf)
+    while pos < n:
+        w, pos = read_word(buf, pos)
+        if w == b"</s>":
+            if cache_eos:
+                stream.append(0)
+                offs.append(len(stream))
+                trigger = 0
+        else:
+            if trigger == msl:
+                stream.append(0)
+                offs.append(len(stream))
+                trigger = 0
+            else:
+                trigger += 1
+            stream.append(int(w))
+    offs.pop()
+    stream.append(0)
+    return np.array(stream, np.int32), np.array(offs, np.int64), int(tw)
+
+
 def corpus_from_text(buf: bytes, *, min_count: int, msl: int, cache_eos: bool) -> Corpus:
     words, counts, tw = learn_vocab(buf, min_count)
     stream, chunk_off = create_stream(buf, words, msl, cache_eos)

@@ -132,8 +132,18 @@ def run_case(name: str, text: bytes, flags: list[str]):
         syn0 = np.stack(rows)
         threads = sorted(f for f in os.listdir(dump) if f.endswith(".bin"))
         per = [parse_dump(os.path.join(dump, f)) for f in threads]
+        # The reference's corpus cache and interpreted corpus for the same flags
+        # (preprocessing only: no -output).
+        cache = os.path.join(tmp, "out.cache")
+        interp = os.path.join(tmp, "out.corpus")
+        pre = [HARNESS, "-train", corpus, "-debug", "0", "-save-corpus-cache", cache,
+               "-save-corpus", interp] + [f for f in flags if f not in ("-output",)]
+        subprocess.run(pre, capture_output=True, check=True, text=True)
+        cache_bytes = open(cache, "rb").read()
         arrays = {
             "corpus": np.frombuffer(text, np.uint8),
+            "corpus_cache": np.frombuffer(cache_bytes, np.uint8),
+            "corpus_text_sha256": np.array(hashlib.sha256(open(interp, "rb").read()).hexdigest()),
             "flags": np.array(" ".join(flags)),
             "vocab_words": np.array([w.decode("latin-1") for w in words]),
             "vocab_counts": np.array(counts, np.uint32),
@@ -150,6 +160,27 @@ def run_case(name: str, text: bytes, flags: list[str]):
             assert V < 32768
             arrays[f"t{t}_ids"] = ids.astype(np.int16)
             arrays[f"t{t}_negs"] = negs.astype(np.int16)
+        # The same run fed from the reference's own vocabulary and corpus cache
+        # files (ReadVocab + readCorpusCache, improved_driver_functions.cpp:167-196,
+        # 320-401): its batches, and the cache it writes back out.
+        dump2 = os.path.join(tmp, "dump_cache")
+        os.mkdir(dump2)
+        recache = os.path.join(tmp, "re.cache")
+        cmd2 = [HARNESS, "-read-vocab", vocab, "-read-corpus-cache", cache, "-output", vec, "-debug", "0",
+                "-binary", "1", "-streams", "1", "-kernel-batch-size", "4",
+                "-save-corpus-cache", recache] + flags
+        r2 = subprocess.run(cmd2, env=dict(os.environ, FW2V_REF_DUMP_DIR=dump2), capture_output=True,
+                            check=True, text=True)
+        ow2 = [ln for ln in r2.stdout.splitlines() if ln.startswith("Overall Words:")]
+        arrays["cache_overall_words"] = np.array(int(ow2[0].split(":")[1]), np.int64)
+        arrays["recache_sha256"] = np.array(hashlib.sha256(open(recache, "rb").read()).hexdigest())
+        per2 = [parse_dump(os.path.join(dump2, f)) for f in sorted(os.listdir(dump2))]
+        for t, (lens, alphas, ids, negs) in enumerate(per2):
+            arrays[f"c{t}_lens"] = lens
+            arrays[f"c{t}_alphas"] = alphas
+            arrays[f"c{t}_ids"] = ids.astype(np.int16)
+            arrays[f"c{t}_negs"] = negs.astype(np.int16)
+        arrays["cache_n_threads"] = np.array(len(per2), np.int32)
         np.savez_compressed(os.path.join(OUT, name + ".npz"), **arrays)
         print(f"{name}: V={V} overall_words={overall_words} threads={len(per)} "
               f"entries={[len(x[0]) for x in per]}")

@@ -40,4 +40,12 @@ def load(name: str) -> dict:
          "ids": g[f"t{t}_ids"].astype(np.int32), "negs": g[f"t{t}_negs"].astype(np.int32)}
         for t in range(T)
     ]
+    C = int(g["cache_n_threads"])
+    g["cache_threads_out"] = [
+        {"lens": g[f"c{t}_lens"], "alphas": g[f"c{t}_alphas"],
+         "ids": g[f"c{t}_ids"].astype(np.int32), "negs": g[f"c{t}_negs"].astype(np.int32)}
+        for t in range(C)
+    ]
+    g["cache_text"] = g["corpus_cache"].tobytes()
+    g["vocab_text"] = "".join(f"{w} {c}\n" for w, c in zip(g["vocab_words"], g["vocab_counts"])).encode("latin-1")
     return g

@@ -95,3 +95,30 @@ def test_unigram_quirk_word1_takes_eos_share():
     # runs reproduce the literal table
     for j, w in enumerate(words):
         assert np.all(table[starts[j]:starts[j + 1]] == w)
+
+
+def _match_streams(out, ref, check_alpha):
+    unmatched = list(range(len(ref)))
+    for per_epoch in out:
+        lens, ids = _concat(per_epoch, "lens"), _concat(per_epoch, "ids")
+        hit = [t for t in unmatched if np.array_equal(ref[t]["lens"], lens)
+               and np.array_equal(ref[t]["ids"], ids)]
+        assert hit, "a stream differs from every reference thread"
+        unmatched.remove(hit[0])
+        np.testing.assert_array_equal(_concat(per_epoch, "negs"), ref[hit[0]]["negs"])
+        if check_alpha:
+            np.testing.assert_array_equal(_concat(per_epoch, "alphas"), ref[hit[0]]["alphas"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_cache_fed_sampler_matches_reference(name):
+    """The reference run from its own vocabulary file and corpus cache."""
+    g = load(name)
+    c = g["cfg"]
+    words, counts, _ = O.read_vocab(g["vocab_text"], c["min_count"])
+    stream, offs, tw = O.read_corpus_cache(g["cache_text"], c["msl"], c["cache_eos"])
+    corpus = O.Corpus(stream, offs, counts, words, tw)
+    out = O.sample_streams(corpus, threads=c["threads"], msl=c["msl"], negative=c["negative"],
+                           epochs=c["iter"], alpha0=c["alpha"], sample=c["sample"])
+    _match_streams(out, g["cache_threads_out"], c["threads"] == 1)
+    assert sum(e.words_read for p in out for e in p) == int(g["cache_overall_words"])
