@@ -19,7 +19,7 @@ namespace fw2v {
 cudaError_t launch_sampler(const SamplerParams& p, int64_t max_region, int64_t* entry_prefix, cudaStream_t st);
 cudaError_t launch_train(const TrainParams& p, int num_sms, cudaStream_t st);
 cudaError_t launch_heldout(const TrainParams& p, double* loss, unsigned long long* pairs, cudaStream_t st);
-cudaError_t launch_init_tables(float* syn0, int64_t V, int d, int64_t pitch, const uint32_t* d_counts,
+cudaError_t launch_init_tables(void* syn0, bool bf16, int64_t V, int d, int64_t pitch, const uint32_t* d_counts,
                                float sample, uint64_t train_words, int32_t* keep_thr, const int64_t* d_firsts,
                                int n_firsts, int32_t* unigram, int64_t table_size, cudaStream_t st);
 size_t train_smem_bytes(int window, int64_t pitch, int warps, int r);
@@ -59,8 +59,10 @@ struct fw2v_handle {
   int64_t V = 0;
   uint64_t train_words = 0;
   int64_t pitch = 0;
-  float* syn0 = nullptr;
-  float* syn1neg = nullptr;
+  void* syn0 = nullptr;  // float, or uint16 bfloat16 bits with FW2V_BF16
+  void* syn1neg = nullptr;
+  size_t elem = 4;        // bytes per table element
+  uint64_t launches = 0;  // training launches so far (stochastic-rounding seeds)
   int32_t* keep_thr = nullptr;
   int32_t* unigram = nullptr;
   uint64_t* jump_a = nullptr;
@@ -89,7 +91,7 @@ struct fw2v_handle {
 
   int* error_flag = nullptr;
   unsigned long long* work_counter = nullptr;
-  float* orig_scratch = nullptr;
+  void* orig_scratch = nullptr;
   int64_t scratch_warps = 0;
 
   int epochs_done = 0;
@@ -118,6 +120,11 @@ fw2v_status fail(fw2v_handle* h, fw2v_status s, const char* fmt, ...) {
                   "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);    \
     }                                                                                       \
   } while (0)
+
+void dfree_v(void*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
 
 template <typename T>
 void dfree(T*& p) {
@@ -160,6 +167,8 @@ TrainParams base_train_params(fw2v_handle* h) {
   p.exp_table = h->exp_table;
   p.orig_scratch = h->orig_scratch;
   p.scratch_warps = h->scratch_warps;
+  p.bf16 = h->cfg.precision == FW2V_BF16;
+  p.sr_seed = mix64(0x5EEDF00DULL + h->launches);
   return p;
 }
 
@@ -226,7 +235,7 @@ fw2v_status fw2v_create(const fw2v_config* cfg, fw2v_handle** out) {
       !(c.alpha > 0) || !(c.sample >= 0) || (c.sigmoid != 0 && c.sigmoid != 1) ||
       (c.precision != FW2V_FP32 && c.precision != FW2V_BF16))
     return FW2V_ERR_ARGUMENT;
-  if (c.precision == FW2V_BF16) return FW2V_ERR_ARGUMENT;
+  if (c.precision == FW2V_BF16 && c.layer_size > 384) return FW2V_ERR_ARGUMENT;
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n <= c.device || c.device < 0) return FW2V_ERR_NO_DEVICE;
   cudaDeviceProp prop;
@@ -236,6 +245,7 @@ fw2v_status fw2v_create(const fw2v_config* cfg, fw2v_handle** out) {
   if (train_smem_bytes(c.window, P, 1, 8) > (size_t)prop.sharedMemPerBlockOptin) return FW2V_ERR_ARGUMENT;
   fw2v_handle* h = new fw2v_handle();
   h->cfg = c;
+  h->elem = c.precision == FW2V_BF16 ? 2 : 4;
   h->num_sms = prop.multiProcessorCount;
   h->pitch = P;
   auto cleanup = [&](fw2v_status s) {
@@ -253,7 +263,7 @@ fw2v_status fw2v_create(const fw2v_config* cfg, fw2v_handle** out) {
       dalloc(h->exp_table, kExpTableSize) != cudaSuccess)
     return cleanup(FW2V_ERR_NOMEM);
   h->scratch_warps = train_scratch_warps(h->num_sms);
-  if (dalloc(h->orig_scratch, (size_t)h->scratch_warps * (2 * c.window + 1) * P) != cudaSuccess)
+  if (cudaMalloc(&h->orig_scratch, (size_t)h->scratch_warps * (2 * c.window + 1) * P * h->elem) != cudaSuccess)
     return cleanup(FW2V_ERR_NOMEM);
   // LCG jump-ahead table for up to 32 tokens of 1+K steps each.
   const int n_jump = 32 * (1 + c.negative) + 1;
@@ -281,7 +291,7 @@ void fw2v_destroy(fw2v_handle* h) {
   if (!h) return;
   cudaSetDevice(h->cfg.device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  dfree(h->syn0); dfree(h->syn1neg); dfree(h->keep_thr); dfree(h->unigram); dfree(h->exp_table);
+  dfree_v(h->syn0); dfree_v(h->syn1neg); dfree(h->keep_thr); dfree(h->unigram); dfree(h->exp_table);
   dfree(h->jump_a); dfree(h->jump_c);
   dfree(h->stream_ids); dfree(h->chunk_off); dfree(h->chunk_base); dfree(h->stream_base);
   if (h->sstream) cudaStreamSynchronize(h->sstream);
@@ -294,7 +304,7 @@ void fw2v_destroy(fw2v_handle* h) {
       if (*e) cudaEventDestroy(*e);
   }
   if (h->sstream) cudaStreamDestroy(h->sstream);
-  dfree(h->error_flag); dfree(h->work_counter); dfree(h->orig_scratch);
+  dfree(h->error_flag); dfree(h->work_counter); dfree_v(h->orig_scratch);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -308,12 +318,14 @@ fw2v_status fw2v_set_vocab(fw2v_handle* h, const uint32_t* counts, int64_t V, ui
   const int64_t P = h->pitch;
   h->V = V;
   h->train_words = train_words;
-  CK(h, dalloc(h->syn0, (size_t)V * P));
-  CK(h, dalloc(h->syn1neg, (size_t)V * P));
+  dfree_v(h->syn0);
+  dfree_v(h->syn1neg);
+  CK(h, cudaMalloc(&h->syn0, (size_t)V * P * h->elem));
+  CK(h, cudaMalloc(&h->syn1neg, (size_t)V * P * h->elem));
   CK(h, dalloc(h->keep_thr, V));
   CK(h, dalloc(h->unigram, kUnigramTableSize));
-  CK(h, cudaMemsetAsync(h->syn0, 0, (size_t)V * P * sizeof(float), h->stream));
-  CK(h, cudaMemsetAsync(h->syn1neg, 0, (size_t)V * P * sizeof(float), h->stream));
+  CK(h, cudaMemsetAsync(h->syn0, 0, (size_t)V * P * h->elem, h->stream));
+  CK(h, cudaMemsetAsync(h->syn1neg, 0, (size_t)V * P * h->elem, h->stream));
   std::vector<int64_t> firsts((size_t)V - 1);
   fw2v_unigram_firsts(counts, V, kUnigramTableSize, firsts.data());
   uint32_t* d_counts = nullptr;
@@ -322,7 +334,7 @@ fw2v_status fw2v_set_vocab(fw2v_handle* h, const uint32_t* counts, int64_t V, ui
   CK(h, dalloc(d_firsts, V - 1));
   CK(h, cudaMemcpyAsync(d_counts, counts, V * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaMemcpyAsync(d_firsts, firsts.data(), (V - 1) * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
-  CK(h, launch_init_tables(h->syn0, V, d, P, d_counts, h->cfg.sample, train_words, h->keep_thr, d_firsts,
+  CK(h, launch_init_tables(h->syn0, h->elem == 2, V, d, P, d_counts, h->cfg.sample, train_words, h->keep_thr, d_firsts,
                            (int)(V - 1), h->unigram, kUnigramTableSize, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
   dfree(d_counts);
@@ -567,6 +579,7 @@ static fw2v_status launch_epoch_train(fw2v_handle* h, SampleBuf** used) {
   CK(h, cudaEventRecord(h->ev[1], h->stream));
   CK(h, cudaMemsetAsync(h->work_counter, 0, sizeof(unsigned long long), h->stream));
   CK(h, launch_train(p, h->num_sms, h->stream));
+  h->launches++;
   CK(h, cudaEventRecord(h->ev[2], h->stream));
   CK(h, cudaEventRecord(b.freed, h->stream));
   b.used = true;
@@ -647,32 +660,52 @@ fw2v_status fw2v_words_trained(fw2v_handle* h, uint64_t* words) {
   return FW2V_OK;
 }
 
-static fw2v_status copy_table(fw2v_handle* h, float* dst, const float* src, int64_t stride, bool to_host) {
-  if (!h || !dst || stride < h->cfg.layer_size) return fail(h, FW2V_ERR_ARGUMENT, "table copy: bad stride");
+static fw2v_status copy_table(fw2v_handle* h, void* dev, float* host, int64_t stride, bool to_host) {
+  if (!h || !host || stride < h->cfg.layer_size) return fail(h, FW2V_ERR_ARGUMENT, "table copy: bad stride");
   if (h->V == 0) return fail(h, FW2V_ERR_STATE, "tables not allocated");
   CK(h, cudaSetDevice(h->cfg.device));
-  const size_t w = (size_t)h->cfg.layer_size * sizeof(float);
-  if (to_host) {
-    CK(h, cudaMemcpy2DAsync(dst, stride * sizeof(float), src, h->pitch * sizeof(float), w, h->V,
-                            cudaMemcpyDeviceToHost, h->stream));
-  } else {
-    CK(h, cudaMemcpy2DAsync(dst, h->pitch * sizeof(float), src, stride * sizeof(float), w, h->V,
-                            cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaStreamSynchronize(h->sstream));
+  const int d = h->cfg.layer_size;
+  if (h->elem == 4) {
+    const size_t w = (size_t)d * sizeof(float);
+    if (to_host)
+      CK(h, cudaMemcpy2DAsync(host, stride * sizeof(float), dev, h->pitch * sizeof(float), w, h->V,
+                              cudaMemcpyDeviceToHost, h->stream));
+    else
+      CK(h, cudaMemcpy2DAsync(dev, h->pitch * sizeof(float), host, stride * sizeof(float), w, h->V,
+                              cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return FW2V_OK;
   }
-  CK(h, cudaStreamSynchronize(h->stream));
+  // bfloat16 tables: widen (exact) on the way out, round to nearest on the way in
+  std::vector<uint16_t> tmp((size_t)h->V * d);
+  const size_t w = (size_t)d * sizeof(uint16_t);
+  if (to_host) {
+    CK(h, cudaMemcpy2DAsync(tmp.data(), w, dev, h->pitch * sizeof(uint16_t), w, h->V, cudaMemcpyDeviceToHost,
+                            h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    for (int64_t r = 0; r < h->V; r++)
+      for (int c = 0; c < d; c++) host[r * stride + c] = bf16_value(tmp[(size_t)r * d + c]);
+  } else {
+    for (int64_t r = 0; r < h->V; r++)
+      for (int c = 0; c < d; c++) tmp[(size_t)r * d + c] = bf16_nearest(host[r * stride + c]);
+    CK(h, cudaMemcpy2DAsync(dev, h->pitch * sizeof(uint16_t), tmp.data(), w, w, h->V, cudaMemcpyHostToDevice,
+                            h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+  }
   return FW2V_OK;
 }
 
 fw2v_status fw2v_get_syn0(fw2v_handle* h, float* out, int64_t row_stride) {
-  return copy_table(h, out, h ? h->syn0 : nullptr, row_stride, true);
+  return copy_table(h, h ? h->syn0 : nullptr, out, row_stride, true);
 }
 fw2v_status fw2v_get_syn1neg(fw2v_handle* h, float* out, int64_t row_stride) {
-  return copy_table(h, out, h ? h->syn1neg : nullptr, row_stride, true);
+  return copy_table(h, h ? h->syn1neg : nullptr, out, row_stride, true);
 }
 fw2v_status fw2v_set_tables(fw2v_handle* h, const float* syn0, const float* syn1neg, int64_t row_stride) {
   fw2v_status s = FW2V_OK;
-  if (syn0) s = copy_table(h, h ? h->syn0 : nullptr, syn0, row_stride, false);
-  if (s == FW2V_OK && syn1neg) s = copy_table(h, h ? h->syn1neg : nullptr, syn1neg, row_stride, false);
+  if (syn0) s = copy_table(h, h ? h->syn0 : nullptr, const_cast<float*>(syn0), row_stride, false);
+  if (s == FW2V_OK && syn1neg) s = copy_table(h, h ? h->syn1neg : nullptr, const_cast<float*>(syn1neg), row_stride, false);
   return s;
 }
 
@@ -732,6 +765,7 @@ fw2v_status fw2v_train_sentences(fw2v_handle* h, const int32_t* ids, const int32
   p.n_sentences = n;
   CK(h, cudaMemsetAsync(h->work_counter, 0, sizeof(unsigned long long), h->stream));
   CK(h, launch_train(p, h->num_sms, h->stream));
+  h->launches++;
   return check_flag(h, "train_sentences");
 }
 

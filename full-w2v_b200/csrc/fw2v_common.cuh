@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string.h>
 
 namespace fw2v {
 
@@ -33,6 +34,47 @@ __host__ __device__ __forceinline__ Affine lcg_jump(uint64_t n) {
     n >>= 1;
   }
   return res;
+}
+
+// Counter-based random bits for stochastic rounding: a write-back event of a
+// training launch (seed), a sentence (uid) and an event within it (a target
+// row's or a leaving context row's write-back) gives a key; each vector of a
+// row then draws 64 bits from (key, row, vector), 16 per element.
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+__host__ __device__ __forceinline__ uint64_t sr_event_key(uint64_t seed, uint64_t uid, uint64_t event) {
+  return mix64(seed ^ mix64(uid * 0x9E3779B97F4A7C15ULL + event));
+}
+__host__ __device__ __forceinline__ uint64_t sr_vector_bits(uint64_t key, uint64_t row, uint64_t vec) {
+  return mix64(key ^ (row * 0xD6E8FEB86659FD93ULL) ^ (vec + 1));
+}
+// x rounded to bfloat16 up or down with probability proportional to the
+// distance (r16 uniform in [0, 65536)); NaN and infinity round to nearest.
+__host__ __device__ __forceinline__ uint16_t bf16_stochastic(float x, uint32_t r16) {
+  uint32_t b;
+  memcpy(&b, &x, 4);
+  if ((b & 0x7F800000u) == 0x7F800000u) {
+    if (b & 0x007FFFFFu) return (uint16_t)((b >> 16) | 0x40);  // quiet NaN
+    return (uint16_t)(b >> 16);                                // infinity
+  }
+  return (uint16_t)((b + (r16 & 0xFFFFu)) >> 16);
+}
+__host__ __device__ __forceinline__ float bf16_value(uint16_t h) {
+  const uint32_t b = (uint32_t)h << 16;
+  float x;
+  memcpy(&x, &b, 4);
+  return x;
+}
+// Round to nearest even (table initialisation and host conversions).
+__host__ __device__ __forceinline__ uint16_t bf16_nearest(float x) {
+  uint32_t b;
+  memcpy(&b, &x, 4);
+  if ((b & 0x7F800000u) == 0x7F800000u) return (uint16_t)((b >> 16) | ((b & 0x007FFFFFu) ? 0x40 : 0));
+  return (uint16_t)((b + 0x7FFFu + ((b >> 16) & 1u)) >> 16);
 }
 
 // Learning-rate refresh (FULL-W2V-driver.cu:188-189) with the global word count
@@ -105,9 +147,9 @@ enum SentenceSource : int {
 };
 
 struct TrainParams {
-  float* syn0;
-  float* syn1neg;
-  int64_t pitch;  // floats per row
+  void* syn0;     // float or bfloat16 (uint16) rows, by the kernel's element type
+  void* syn1neg;
+  int64_t pitch;  // elements per row, also the float stride of shared-memory rows
   int64_t vocab;
   int d, window, negative, sigmoid;
   const int32_t* ids;
@@ -131,10 +173,12 @@ struct TrainParams {
   int deterministic;
   int* error_flag;
   const float* exp_table;
-  // per-warp scratch, (2W+1) * pitch floats for each of scratch_warps warps:
+  // per-warp scratch, (2W+1) * pitch elements for each of scratch_warps warps:
   // the value every ring row had when it entered the window
-  float* orig_scratch;
+  void* orig_scratch;
   int64_t scratch_warps;
+  uint64_t sr_seed;  // stochastic rounding of bfloat16 write-backs
+  int bf16;          // tables hold bfloat16
 };
 
 // Sampler output layout: stream s keeps its kept ids at [stream_base[s],

@@ -84,6 +84,7 @@ extern "C" fw2v_status fw2v_kernel_batch_noalloc(float* syn0, float* syn1neg, co
   p.msl = msl;
   p.work_counter = nullptr;  // static sentence-to-warp assignment
   p.deterministic = 0;
+  p.bf16 = 0;
   p.error_flag = error_word;
   p.exp_table = table;
   p.orig_scratch = scratch;

@@ -81,6 +81,7 @@ extern "C" fw2v_status fw2v_kernel_batch(float* syn0, float* syn1neg, const int3
   p.msl = msl;
   p.work_counter = nullptr;
   p.deterministic = 0;
+  p.bf16 = 0;
   void* addr = nullptr;
   if (cudaGetSymbolAddress(&addr, g_seam_error) != cudaSuccess) return FW2V_ERR_CUDA;
   p.error_flag = (int*)addr;

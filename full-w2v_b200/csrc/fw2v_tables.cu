@@ -19,17 +19,21 @@ namespace fw2v {
 
 // improved_driver_functions.cpp:27-31; element i = row*d + c uses the
 // (i+1)-th LCG state from seed 1.  One thread per row, started by jump-ahead.
-__global__ void init_syn0_kernel(float* syn0, int64_t V, int d, int64_t pitch) {
+// Bfloat16 tables take the FP32 value rounded to nearest.
+template <typename T>
+__global__ void init_syn0_kernel(T* syn0, int64_t V, int d, int64_t pitch) {
   const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (row >= V) return;
   const Affine j = lcg_jump((uint64_t)row * (uint64_t)d);
   uint64_t r = j.a * 1ULL + j.c;  // state after row*d steps from seed 1
-  float* out = syn0 + row * pitch;
+  T* out = syn0 + row * pitch;
   const float fd = (float)d;
   for (int c = 0; c < d; c++) {
     r = lcg_next(r);
     const float u = __uint2float_rn((unsigned)(r & 0xFFFF)) / 65536.0f;
-    out[c] = __fdiv_rn(__fsub_rn(u, 0.5f), fd);
+    const float x = __fdiv_rn(__fsub_rn(u, 0.5f), fd);
+    if constexpr (sizeof(T) == 4) out[c] = x;
+    else out[c] = bf16_nearest(x);
   }
 }
 
@@ -106,12 +110,13 @@ extern "C" int fw2v_unigram_firsts(const uint32_t* counts, int64_t V, int64_t si
 
 namespace fw2v {
 
-cudaError_t launch_init_tables(float* syn0, int64_t V, int d, int64_t pitch, const uint32_t* d_counts,
+cudaError_t launch_init_tables(void* syn0, bool bf16, int64_t V, int d, int64_t pitch, const uint32_t* d_counts,
                                float sample, uint64_t train_words, int32_t* keep_thr,
                                const int64_t* d_firsts, int n_firsts, int32_t* unigram,
                                int64_t table_size, cudaStream_t st) {
   const int b = 256;
-  init_syn0_kernel<<<(unsigned)((V + b - 1) / b), b, 0, st>>>(syn0, V, d, pitch);
+  if (bf16) init_syn0_kernel<<<(unsigned)((V + b - 1) / b), b, 0, st>>>((uint16_t*)syn0, V, d, pitch);
+  else init_syn0_kernel<<<(unsigned)((V + b - 1) / b), b, 0, st>>>((float*)syn0, V, d, pitch);
   subsample_kernel<<<(unsigned)((V + b - 1) / b), b, 0, st>>>(d_counts, V, sample, train_words, keep_thr);
   unigram_fill_kernel<<<148 * 16, 256, 0, st>>>(d_firsts, n_firsts, unigram, table_size);
   return cudaGetLastError();

@@ -3,20 +3,29 @@
 
 namespace fw2v {
 
-extern template cudaError_t launch_r<2, 1, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<2, 1, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 1, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 1, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 2, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 2, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 3, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 3, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 4, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 4, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 6, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 6, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 8, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
-extern template cudaError_t launch_r<4, 8, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<float, 2, 1, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<float, 2, 1, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<float, 4, 1, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<float, 4, 1, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<float, 4, 2, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<float, 4, 2, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<float, 4, 3, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<float, 4, 3, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<float, 4, 4, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<float, 4, 4, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<float, 4, 6, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<float, 4, 6, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<float, 4, 8, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<float, 4, 8, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<bf16_t, 2, 1, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<bf16_t, 2, 1, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<bf16_t, 4, 1, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<bf16_t, 4, 1, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<bf16_t, 4, 2, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<bf16_t, 4, 2, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<bf16_t, 4, 3, 0>(const TrainParams&, int, int, size_t, cudaStream_t);
+extern template cudaError_t launch_r<bf16_t, 4, 3, 1>(const TrainParams&, int, int, size_t, cudaStream_t);
+
 
 
 struct LaunchShape {
@@ -51,30 +60,52 @@ size_t train_smem_bytes(int window, int64_t pitch, int warps, int r) {
 // hold (64 per SM at most).
 int64_t train_scratch_warps(int num_sms) { return (int64_t)num_sms * 64; }
 
+// Table type and sigmoid mode of a launch; bfloat16 tables cover rows of up to
+// 384 elements (three 4-float vectors per lane).
+template <int VEC, int NV>
+static cudaError_t launch_rt(const TrainParams& p, int r, int num_sms, size_t smem, cudaStream_t st) {
+  if (p.bf16) {
+    if constexpr (NV <= 3) {
+      return p.sigmoid == 0 ? launch_r<bf16_t, VEC, NV, 0>(p, r, num_sms, smem, st)
+                            : launch_r<bf16_t, VEC, NV, 1>(p, r, num_sms, smem, st);
+    } else {
+      return cudaErrorInvalidValue;
+    }
+  }
+  return p.sigmoid == 0 ? launch_r<float, VEC, NV, 0>(p, r, num_sms, smem, st)
+                        : launch_r<float, VEC, NV, 1>(p, r, num_sms, smem, st);
+}
+
 cudaError_t launch_train(const TrainParams& p, int num_sms, cudaStream_t st) {
   const LaunchShape s = choose_shape(p.d, p.negative);
   const size_t smem = train_smem_bytes(p.window, p.pitch, p.deterministic ? 1 : kWarpsPerBlock, s.r);
-  if (s.vec == 2) return p.sigmoid == 0 ? launch_r<2, 1, 0>(p, s.r, num_sms, smem, st) : launch_r<2, 1, 1>(p, s.r, num_sms, smem, st);
+  if (s.vec == 2) return launch_rt<2, 1>(p, s.r, num_sms, smem, st);
   switch (s.nv) {
-    case 1: return p.sigmoid == 0 ? launch_r<4, 1, 0>(p, s.r, num_sms, smem, st) : launch_r<4, 1, 1>(p, s.r, num_sms, smem, st);
-    case 2: return p.sigmoid == 0 ? launch_r<4, 2, 0>(p, s.r, num_sms, smem, st) : launch_r<4, 2, 1>(p, s.r, num_sms, smem, st);
-    case 3: return p.sigmoid == 0 ? launch_r<4, 3, 0>(p, s.r, num_sms, smem, st) : launch_r<4, 3, 1>(p, s.r, num_sms, smem, st);
-    case 4: return p.sigmoid == 0 ? launch_r<4, 4, 0>(p, s.r, num_sms, smem, st) : launch_r<4, 4, 1>(p, s.r, num_sms, smem, st);
-    case 6: return p.sigmoid == 0 ? launch_r<4, 6, 0>(p, s.r, num_sms, smem, st) : launch_r<4, 6, 1>(p, s.r, num_sms, smem, st);
-    default: return p.sigmoid == 0 ? launch_r<4, 8, 0>(p, s.r, num_sms, smem, st) : launch_r<4, 8, 1>(p, s.r, num_sms, smem, st);
+    case 1: return launch_rt<4, 1>(p, s.r, num_sms, smem, st);
+    case 2: return launch_rt<4, 2>(p, s.r, num_sms, smem, st);
+    case 3: return launch_rt<4, 3>(p, s.r, num_sms, smem, st);
+    case 4: return launch_rt<4, 4>(p, s.r, num_sms, smem, st);
+    case 6: return launch_rt<4, 6>(p, s.r, num_sms, smem, st);
+    default: return launch_rt<4, 8>(p, s.r, num_sms, smem, st);
   }
+}
+
+template <int VEC, int NV>
+static void heldout_t(const TrainParams& p, double* loss, unsigned long long* pairs, int blocks, cudaStream_t st) {
+  if (p.bf16) heldout_loss_kernel<bf16_t, VEC, NV><<<blocks, 128, 0, st>>>(p, loss, pairs);
+  else heldout_loss_kernel<float, VEC, NV><<<blocks, 128, 0, st>>>(p, loss, pairs);
 }
 
 cudaError_t launch_heldout(const TrainParams& p, double* loss, unsigned long long* pairs, cudaStream_t st) {
   const LaunchShape s = choose_shape(p.d, p.negative);
   const int blocks = 148 * 8;
-  if (s.vec == 2) heldout_loss_kernel<2, 1><<<blocks, 128, 0, st>>>(p, loss, pairs);
-  else if (s.nv == 1) heldout_loss_kernel<4, 1><<<blocks, 128, 0, st>>>(p, loss, pairs);
-  else if (s.nv == 2) heldout_loss_kernel<4, 2><<<blocks, 128, 0, st>>>(p, loss, pairs);
-  else if (s.nv == 3) heldout_loss_kernel<4, 3><<<blocks, 128, 0, st>>>(p, loss, pairs);
-  else if (s.nv == 4) heldout_loss_kernel<4, 4><<<blocks, 128, 0, st>>>(p, loss, pairs);
-  else if (s.nv == 6) heldout_loss_kernel<4, 6><<<blocks, 128, 0, st>>>(p, loss, pairs);
-  else heldout_loss_kernel<4, 8><<<blocks, 128, 0, st>>>(p, loss, pairs);
+  if (s.vec == 2) heldout_t<2, 1>(p, loss, pairs, blocks, st);
+  else if (s.nv == 1) heldout_t<4, 1>(p, loss, pairs, blocks, st);
+  else if (s.nv == 2) heldout_t<4, 2>(p, loss, pairs, blocks, st);
+  else if (s.nv == 3) heldout_t<4, 3>(p, loss, pairs, blocks, st);
+  else if (s.nv == 4) heldout_t<4, 4>(p, loss, pairs, blocks, st);
+  else if (s.nv == 6) heldout_t<4, 6>(p, loss, pairs, blocks, st);
+  else heldout_t<4, 8>(p, loss, pairs, blocks, st);
   return cudaGetLastError();
 }
 

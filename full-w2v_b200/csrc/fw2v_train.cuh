@@ -31,7 +31,10 @@
 // the sentence.  The reference's warm-up/cool-down deviations at sentence edges
 // are not reproduced.
 #pragma once
+#include <cuda_bf16.h>
+
 #include <cstdio>
+#include <type_traits>
 #include <utility>
 
 #include "fw2v_common.cuh"
@@ -233,6 +236,104 @@ __device__ __forceinline__ void row_add_delta(float* row, const Row<VEC, NV>& a,
   }
 }
 
+// ---- bfloat16 tables: FP32 math, rows converted on load, stochastic-rounded
+// write-back.  The table type only changes these helpers; everything between
+// a row's load and its write-back is FP32. ----
+using bf16_t = __nv_bfloat16;
+
+template <int VEC, int NV>
+__device__ __forceinline__ void row_load_global(Row<VEC, NV>& r, const bf16_t* row, int lane, int d) {
+  const uint16_t* h = reinterpret_cast<const uint16_t*>(row);
+#pragma unroll
+  for (int i = 0; i < NV; i++) {
+    const int e = (i * 32 + lane) * VEC;
+    if (e + VEC <= d) {
+      if constexpr (VEC == 4) {
+        const uint2 t = __ldcg(reinterpret_cast<const uint2*>(h + e));
+        r.x[i][0] = bf16_value((uint16_t)t.x); r.x[i][1] = bf16_value((uint16_t)(t.x >> 16));
+        r.x[i][2] = bf16_value((uint16_t)t.y); r.x[i][3] = bf16_value((uint16_t)(t.y >> 16));
+      } else {
+        const unsigned t = __ldcg(reinterpret_cast<const unsigned*>(h + e));
+        r.x[i][0] = bf16_value((uint16_t)t); r.x[i][1] = bf16_value((uint16_t)(t >> 16));
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < VEC; j++) r.x[i][j] = e + j < d ? bf16_value(__ldcg(h + e + j)) : 0.0f;
+    }
+  }
+}
+
+// row = SR(row + (a - b)) per element, 16 random bits each from the event key:
+// a compare-and-swap loop per vector (64-bit for 4 elements, 32-bit for 2,
+// 16-bit per element of a vector straddling d).  Lost races retry with the
+// current value; after 64 failed attempts the update is dropped (a Hogwild
+// lost update) so that the loop always ends.
+template <int VEC, int NV>
+__device__ __forceinline__ void row_add_delta(bf16_t* row, const Row<VEC, NV>& a, const Row<VEC, NV>& b, int lane,
+                                              int d, uint64_t key, uint64_t row_id) {
+  uint16_t* h = reinterpret_cast<uint16_t*>(row);
+#pragma unroll
+  for (int i = 0; i < NV; i++) {
+    const int e = (i * 32 + lane) * VEC;
+    if (e >= d) continue;
+    const uint64_t bits = sr_vector_bits(key, row_id, (uint64_t)(e / VEC));
+    float dl[VEC];
+#pragma unroll
+    for (int j = 0; j < VEC; j++) dl[j] = __fsub_rn(a.x[i][j], b.x[i][j]);
+    if (e + VEC <= d) {
+      if constexpr (VEC == 4) {
+        unsigned long long* addr = reinterpret_cast<unsigned long long*>(h + e);
+        unsigned long long old = __ldcg(addr);
+        for (int it = 0; it < 64; it++) {
+          unsigned long long nv = 0;
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            const float cur = bf16_value((uint16_t)(old >> (16 * j)));
+            nv |= (unsigned long long)bf16_stochastic(__fadd_rn(cur, dl[j]), (uint32_t)(bits >> (16 * j))) << (16 * j);
+          }
+          const unsigned long long prev = atomicCAS(addr, old, nv);
+          if (prev == old) break;
+          old = prev;
+        }
+      } else {
+        unsigned* addr = reinterpret_cast<unsigned*>(h + e);
+        unsigned old = __ldcg(addr);
+        for (int it = 0; it < 64; it++) {
+          unsigned nv = 0;
+#pragma unroll
+          for (int j = 0; j < 2; j++) {
+            const float cur = bf16_value((uint16_t)(old >> (16 * j)));
+            nv |= (unsigned)bf16_stochastic(__fadd_rn(cur, dl[j]), (uint32_t)(bits >> (16 * j))) << (16 * j);
+          }
+          const unsigned prev = atomicCAS(addr, old, nv);
+          if (prev == old) break;
+          old = prev;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < VEC; j++) {
+        if (e + j >= d) continue;
+        unsigned short* addr = reinterpret_cast<unsigned short*>(h + e + j);
+        unsigned short old = __ldcg(addr);
+        for (int it = 0; it < 64; it++) {
+          const unsigned short nv = bf16_stochastic(__fadd_rn(bf16_value(old), dl[j]), (uint32_t)(bits >> (16 * j)));
+          const unsigned short prev = atomicCAS(addr, old, nv);
+          if (prev == old) break;
+          old = prev;
+        }
+      }
+    }
+  }
+}
+
+// The FP32 table takes exact atomic adds; the key is unused.
+template <int VEC, int NV>
+__device__ __forceinline__ void row_add_delta(float* row, const Row<VEC, NV>& a, const Row<VEC, NV>& b, int lane,
+                                              int d, uint64_t, uint64_t) {
+  row_add_delta(row, a, b, lane, d);
+}
+
 template <int VEC, int NV>
 __device__ __forceinline__ float row_dot(const Row<VEC, NV>& a, const Row<VEC, NV>& b) {
   float p = __fmul_rn(a.x[0][0], b.x[0][0]);
@@ -281,6 +382,7 @@ struct Sentence {
   int64_t start;
   int32_t len;
   float alpha;
+  int64_t uid;  // the sentence's number in its launch (stochastic-rounding key)
 };
 
 __device__ __forceinline__ int64_t total_sentences(const TrainParams& p) {
@@ -290,6 +392,7 @@ __device__ __forceinline__ int64_t total_sentences(const TrainParams& p) {
 
 __device__ __forceinline__ Sentence fetch_sentence(const TrainParams& p, int64_t w) {
   Sentence s;
+  s.uid = w;
   if (p.source == kSourceEpoch) {
     int lo = 0, hi = p.threads - 1;  // last stream with prefix <= w
     while (lo < hi) {
@@ -400,6 +503,80 @@ __device__ __forceinline__ void row_store_global(const Row<VEC, NV>& r, float* r
   }
 }
 
+template <int VEC, int NV>
+__device__ __forceinline__ void row_store_global(const Row<VEC, NV>& r, bf16_t* row, int lane, int d) {
+  uint16_t* h = reinterpret_cast<uint16_t*>(row);
+#pragma unroll
+  for (int i = 0; i < NV; i++) {
+    const int e = (i * 32 + lane) * VEC;
+    if (e + VEC <= d) {
+      if constexpr (VEC == 4) {
+        uint2 t;
+        t.x = (unsigned)bf16_nearest(r.x[i][0]) | ((unsigned)bf16_nearest(r.x[i][1]) << 16);
+        t.y = (unsigned)bf16_nearest(r.x[i][2]) | ((unsigned)bf16_nearest(r.x[i][3]) << 16);
+        __stcg(reinterpret_cast<uint2*>(h + e), t);
+      } else {
+        __stcg(reinterpret_cast<unsigned*>(h + e),
+               (unsigned)bf16_nearest(r.x[i][0]) | ((unsigned)bf16_nearest(r.x[i][1]) << 16));
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < VEC; j++)
+        if (e + j < d) h[e + j] = bf16_nearest(r.x[i][j]);
+    }
+  }
+}
+
+// Staging copies of a bfloat16 row keep its 2-byte elements (byte offset e*2).
+template <int VEC, int NV>
+__device__ __forceinline__ void cp_row(uint32_t dst, const bf16_t* src, const LaneMap<VEC, NV>& m, int d) {
+  const uint16_t* h = reinterpret_cast<const uint16_t*>(src);
+#pragma unroll
+  for (int i = 0; i < NV; i++) {
+    if (!m.ok[i]) continue;
+    const int e = (int)(m.off[i] / 4);
+    const uint32_t da = dst + (uint32_t)e * 2u;
+    if (e + VEC <= d) {
+      if constexpr (VEC == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(da), "l"(h + e) : "memory");
+      else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(da), "l"(h + e) : "memory");
+    } else {
+#pragma unroll
+      for (int j = 0; j < VEC; j++) {
+        const unsigned short v = e + j < d ? __ldcg(h + e + j) : (unsigned short)0;
+        asm volatile("st.shared.u16 [%0], %1;" ::"r"(da + 2u * j), "h"(v) : "memory");
+      }
+    }
+  }
+}
+
+template <int VEC, int NV>
+__device__ __forceinline__ void lds_row_bf16(Row<VEC, NV>& r, uint32_t row, const LaneMap<VEC, NV>& m) {
+#pragma unroll
+  for (int i = 0; i < NV; i++) {
+    unsigned a = 0, b = 0;
+    const uint32_t at = row + (m.off[i] / 4) * 2u;
+    if (m.ok[i]) {
+      if constexpr (VEC == 4) asm volatile("ld.shared.v2.u32 {%0,%1}, [%2];" : "=r"(a), "=r"(b) : "r"(at));
+      else asm volatile("ld.shared.u32 %0, [%1];" : "=r"(a) : "r"(at));
+    }
+    r.x[i][0] = bf16_value((uint16_t)a);
+    r.x[i][1] = bf16_value((uint16_t)(a >> 16));
+    if constexpr (VEC == 4) {
+      r.x[i][2] = bf16_value((uint16_t)b);
+      r.x[i][3] = bf16_value((uint16_t)(b >> 16));
+    }
+  }
+}
+
+// A staging row written by cp_row, in the table's element type.
+template <typename T, int VEC, int NV>
+__device__ __forceinline__ void lds_staged(Row<VEC, NV>& r, uint32_t row, const LaneMap<VEC, NV>& m) {
+  if constexpr (std::is_same_v<T, float>) lds_row(r, row, m);
+  else lds_row_bf16(r, row, m);
+}
+
 // Shared-memory rows of one warp, each `P` floats.
 template <int R>
 struct WarpRows {
@@ -416,8 +593,8 @@ struct WarpRows {
 //            leaving row's original value).
 //   orig     this warp's global scratch, D rows: the value each slot's row had
 //            when it entered the window (needed for its single write-back).
-template <int VEC, int NV, int R, int SIG>
-__device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* ring, float* orig,
+template <typename T, int VEC, int NV, int R, int SIG>
+__device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* ring, T* orig,
                                const float* table, int lane) {
   constexpr int RP = PadPow2<R>::value;
   const int W = p.window, K = p.negative, D = 2 * W + 1;
@@ -426,8 +603,8 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   const int L = sn.len;
   const int32_t* ids = p.ids + sn.start;
   const int32_t* negs = p.negs + sn.start * (int64_t)K;
-  float* const syn0 = p.syn0;
-  float* const syn1neg = p.syn1neg;
+  T* const syn0 = reinterpret_cast<T*>(p.syn0);
+  T* const syn1neg = reinterpret_cast<T*>(p.syn1neg);
   const float alpha = sn.alpha;
   const bool one_group = K + 1 <= R;
 
@@ -564,7 +741,9 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
             if (k < nt) {
               Row<VEC, NV> o0;
               lds_row(o0, o0_b + (uint32_t)k * row_bytes, lm);
-              row_add_delta(syn1neg + (int64_t)tk * P, o[k], o0, lane, d);
+              row_add_delta(syn1neg + (int64_t)tk * P, o[k], o0, lane, d,
+                            sr_event_key(p.sr_seed, (uint64_t)sn.uid, (uint64_t)w * (K + 1) + (k0 + k)),
+                            (uint64_t)tk);
             }
           }
         } else {
@@ -585,7 +764,9 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
               row_update(sv, so, g);
               sts_row(sv, a, lm);
             }
-            row_add_delta(syn1neg + (int64_t)tk * P, so, so0, lane, d);
+            row_add_delta(syn1neg + (int64_t)tk * P, so, so0, lane, d,
+                          sr_event_key(p.sr_seed, (uint64_t)sn.uid, (uint64_t)w * (K + 1) + (k0 + k)),
+                          (uint64_t)tk);
           }
         }
       }
@@ -596,13 +777,14 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
     if (q_out >= 0) {
       Row<VEC, NV> cur, org;
       lds_row(cur, ring_b + (uint32_t)(q_out % D) * row_bytes, lm);
-      lds_row(org, out_b, lm);
-      row_add_delta(syn0 + (int64_t)id_out * P, cur, org, lane, d);
+      lds_staged<T>(org, out_b, lm);
+      row_add_delta(syn0 + (int64_t)id_out * P, cur, org, lane, d,
+                    sr_event_key(p.sr_seed, (uint64_t)sn.uid, (uint64_t)L * (K + 1) + q_out), (uint64_t)id_out);
     }
     if (id_in >= 0) {
       const int s = q_in % D;
       Row<VEC, NV> enter_row;
-      if (enter_early) lds_row(enter_row, in_b, lm);
+      if (enter_early) lds_staged<T>(enter_row, in_b, lm);
       else row_load_global(enter_row, syn0 + (int64_t)id_in * P, lane, d);
       sts_row(enter_row, ring_b + (uint32_t)s * row_bytes, lm);
       row_store_global(enter_row, orig + s * P, lane, d);
@@ -614,7 +796,9 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
     Row<VEC, NV> cur, org;
     lds_row(cur, ring_b + (uint32_t)s * row_bytes, lm);
     row_load_global(org, orig + s * P, lane, d);
-    row_add_delta(syn0 + (int64_t)__ldg(ids + q) * P, cur, org, lane, d);
+    const int id_q = __ldg(ids + q);
+    row_add_delta(syn0 + (int64_t)id_q * P, cur, org, lane, d,
+                  sr_event_key(p.sr_seed, (uint64_t)sn.uid, (uint64_t)L * (K + 1) + q), (uint64_t)id_q);
   }
 }
 
@@ -625,7 +809,7 @@ struct MinBlocks {
   static constexpr int value = NV == 1 ? 4 : 2;
 };
 
-template <int VEC, int NV, int R, int SIG>
+template <typename T, int VEC, int NV, int R, int SIG>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, MinBlocks<NV>::value) sgns_train_kernel(TrainParams p) {
   extern __shared__ __align__(16) float smem[];
   const float* table = p.exp_table;
@@ -634,13 +818,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MinBlocks<NV>::value) sgn
   const int D = 2 * p.window + 1;
   float* ring = smem + (int64_t)warp * WarpRows<R>::rows(D) * p.pitch;
   const int64_t gwarp = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
-  float* orig = p.orig_scratch + gwarp * D * p.pitch;
+  T* orig = reinterpret_cast<T*>(p.orig_scratch) + gwarp * D * p.pitch;
   const int64_t total = total_sentences(p);
   if (p.deterministic) {
     if (blockIdx.x != 0 || warp != 0) return;
     for (int64_t w = 0; w < total; w++) {
       const Sentence sn = fetch_sentence(p, w);
-      train_sentence<VEC, NV, R, SIG>(p, sn, ring, orig, table, lane);
+      train_sentence<T, VEC, NV, R, SIG>(p, sn, ring, orig, table, lane);
     }
     return;
   }
@@ -649,7 +833,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MinBlocks<NV>::value) sgn
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     for (int64_t w = gwarp; w < total; w += warps) {
       const Sentence sn = fetch_sentence(p, w);
-      train_sentence<VEC, NV, R, SIG>(p, sn, ring, orig, table, lane);
+      train_sentence<T, VEC, NV, R, SIG>(p, sn, ring, orig, table, lane);
     }
     return;
   }
@@ -659,7 +843,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MinBlocks<NV>::value) sgn
     w = __shfl_sync(kFull, w, 0);
     if ((int64_t)w >= total) break;
     const Sentence sn = fetch_sentence(p, (int64_t)w);
-    train_sentence<VEC, NV, R, SIG>(p, sn, ring, orig, table, lane);
+    train_sentence<T, VEC, NV, R, SIG>(p, sn, ring, orig, table, lane);
   }
 }
 
@@ -670,7 +854,7 @@ __device__ __forceinline__ double log_sigmoid(double x) {
   return x >= 0 ? -log1p(exp(-x)) : x - log1p(exp(x));
 }
 
-template <int VEC, int NV>
+template <typename T, int VEC, int NV>
 __global__ void __launch_bounds__(128) heldout_loss_kernel(TrainParams p, double* loss, unsigned long long* pairs) {
   const int lane = threadIdx.x & 31;
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -696,10 +880,10 @@ __global__ void __launch_bounds__(128) heldout_loss_kernel(TrainParams p, double
         const int pos = base + ((r - base) % D + D) % D;
         if (pos == w || pos < 0 || pos >= L) continue;
         Row<VEC, NV> v, o;
-        row_load_global(v, p.syn0 + (int64_t)ids[pos] * P, lane, d);
+        row_load_global(v, reinterpret_cast<const T*>(p.syn0) + (int64_t)ids[pos] * P, lane, d);
         for (int k = 0; k <= K; k++) {
           const int32_t t = k == 0 ? ids[w] : negs[(int64_t)w * K + k - 1];
-          row_load_global(o, p.syn1neg + (int64_t)t * P, lane, d);
+          row_load_global(o, reinterpret_cast<const T*>(p.syn1neg) + (int64_t)t * P, lane, d);
           // FP64 dot: per-lane partial in double, then the xor tree
           double part = 0.0;
 #pragma unroll
@@ -722,9 +906,9 @@ __global__ void __launch_bounds__(128) heldout_loss_kernel(TrainParams p, double
 
 // Launch of one (VEC, NV) shape for any stage count R (instantiated per shape
 // in fw2v_train_<shape>.cu so the shapes compile in parallel).
-template <int VEC, int NV, int R, int SIG>
+template <typename T, int VEC, int NV, int R, int SIG>
 cudaError_t launch_t(const TrainParams& p, int num_sms, size_t smem, cudaStream_t st) {
-  auto kern = sgns_train_kernel<VEC, NV, R, SIG>;
+  auto kern = sgns_train_kernel<T, VEC, NV, R, SIG>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int blocks = 1;
@@ -747,17 +931,17 @@ cudaError_t launch_t(const TrainParams& p, int num_sms, size_t smem, cudaStream_
 
 // Stage counts compiled per shape: rows of up to 3 vectors per lane pipeline
 // up to 8 targets; wider rows (d > 384) sweep targets one at a time.
-template <int VEC, int NV, int SIG>
+template <typename T, int VEC, int NV, int SIG>
 cudaError_t launch_r(const TrainParams& p, int r, int num_sms, size_t smem, cudaStream_t st) {
   if constexpr (NV >= 4) {
-    return launch_t<VEC, NV, 1, SIG>(p, num_sms, smem, st);
+    return launch_t<T, VEC, NV, 1, SIG>(p, num_sms, smem, st);
   } else {
     switch (r) {
-      case 1: return launch_t<VEC, NV, 1, SIG>(p, num_sms, smem, st);
-      case 2: return launch_t<VEC, NV, 2, SIG>(p, num_sms, smem, st);
-      case 4: return launch_t<VEC, NV, 4, SIG>(p, num_sms, smem, st);
-      case 6: return launch_t<VEC, NV, 6, SIG>(p, num_sms, smem, st);
-      default: return launch_t<VEC, NV, 8, SIG>(p, num_sms, smem, st);
+      case 1: return launch_t<T, VEC, NV, 1, SIG>(p, num_sms, smem, st);
+      case 2: return launch_t<T, VEC, NV, 2, SIG>(p, num_sms, smem, st);
+      case 4: return launch_t<T, VEC, NV, 4, SIG>(p, num_sms, smem, st);
+      case 6: return launch_t<T, VEC, NV, 6, SIG>(p, num_sms, smem, st);
+      default: return launch_t<T, VEC, NV, 8, SIG>(p, num_sms, smem, st);
     }
   }
 }

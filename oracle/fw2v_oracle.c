@@ -365,6 +365,125 @@ static double dot_f64(const orc_train_cfg* cfg, const double* a, const double* b
 DEFINE_TRAIN(orc_train_f32, float, dot_f32, grad_f32, UPD_F32, UPD_F32, 0)
 DEFINE_TRAIN(orc_train_f64, double, dot_f64, grad_f64, UPD_F64, UPD_F64, 0)
 
+/* ---- bfloat16 tables (FP32 math, stochastic-rounded write-back) ---- */
+static uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+static uint64_t sr_event_key(uint64_t seed, uint64_t uid, uint64_t event) {
+  return mix64(seed ^ mix64(uid * 0x9E3779B97F4A7C15ULL + event));
+}
+static uint64_t sr_vector_bits(uint64_t key, uint64_t row, uint64_t vec) {
+  return mix64(key ^ (row * 0xD6E8FEB86659FD93ULL) ^ (vec + 1));
+}
+static float bf16_f(uint16_t h) {
+  uint32_t b = (uint32_t)h << 16;
+  float x;
+  memcpy(&x, &b, 4);
+  return x;
+}
+static uint16_t bf16_sr(float x, uint32_t r16) {
+  uint32_t b;
+  memcpy(&b, &x, 4);
+  if ((b & 0x7F800000u) == 0x7F800000u) return (uint16_t)((b >> 16) | ((b & 0x007FFFFFu) ? 0x40 : 0));
+  return (uint16_t)((b + (r16 & 0xFFFFu)) >> 16);
+}
+uint16_t orc_bf16_nearest(float x) {
+  uint32_t b;
+  memcpy(&b, &x, 4);
+  if ((b & 0x7F800000u) == 0x7F800000u) return (uint16_t)((b >> 16) | ((b & 0x007FFFFFu) ? 0x40 : 0));
+  return (uint16_t)((b + 0x7FFFu + ((b >> 16) & 1u)) >> 16);
+}
+
+/* row = SR(row + delta) with the kernel's random bits for (key, row id). */
+static void bf16_writeback(uint16_t* row, const float* delta, int d, int vec, uint64_t key, uint64_t row_id) {
+  for (int e = 0; e < d; e++) {
+    uint64_t bits = sr_vector_bits(key, row_id, (uint64_t)(e / vec));
+    uint32_t r16 = (uint32_t)(bits >> (16 * (e % vec)));
+    row[e] = bf16_sr(bf16_f(row[e]) + delta[e], r16);
+  }
+}
+
+/* Serial SGNS on bfloat16 tables with the kernel's FP32 order (orc_train_f32)
+ * and its stochastic rounding: sentence s is uid s, target k of centre w is
+ * event w*(K+1)+k, the leaving position q is event L*(K+1)+q. */
+int orc_train_bf16(const orc_train_cfg* cfg, uint16_t* syn0, uint16_t* syn1, int64_t V, int64_t n_sent,
+                   const int64_t* starts, const int32_t* lens, const float* alphas, const int32_t* ids,
+                   const int32_t* negs, uint64_t seed) {
+  const int d = cfg->d, W = cfg->window, K = cfg->negative;
+  const int64_t P = cfg->pitch;
+  int32_t maxL = 0;
+  for (int64_t s = 0; s < n_sent; s++)
+    if (lens[s] > maxL) maxL = lens[s];
+  float* cur = (float*)malloc(sizeof(float) * ((size_t)maxL + 1) * d);
+  float* orig = (float*)malloc(sizeof(float) * ((size_t)maxL + 1) * d);
+  float* o = (float*)malloc(sizeof(float) * d);
+  float* o0 = (float*)malloc(sizeof(float) * d);
+  float* delta = (float*)malloc(sizeof(float) * d);
+  int* ctx = (int*)malloc(sizeof(int) * (2 * W + 1));
+  int rc = 0;
+  for (int64_t s = 0; s < n_sent && rc == 0; s++) {
+    const int L = lens[s];
+    if (L <= 0) continue;
+    const int32_t* sid = ids + starts[s];
+    const int32_t* sneg = negs + starts[s] * K;
+    for (int p = 0; p < L; p++)
+      if (sid[p] < 0 || sid[p] >= V) rc = -3;
+    for (int64_t q = 0; q < (int64_t)L * K; q++)
+      if (sneg[q] < 0 || sneg[q] >= V) rc = -3;
+    if (rc) break;
+    int n_enter = W + 1 < L ? W + 1 : L;
+    for (int p = 0; p < n_enter; p++)
+      for (int e = 0; e < d; e++) cur[(int64_t)p * d + e] = orig[(int64_t)p * d + e] = bf16_f(syn0[(int64_t)sid[p] * P + e]);
+    for (int w = 0; w < L; w++) {
+      int n = context_list(w, W, L, ctx);
+      if (n > 0) {
+        for (int k = 0; k <= K; k++) {
+          int32_t t = k == 0 ? sid[w] : sneg[(int64_t)w * K + k - 1];
+          for (int e = 0; e < d; e++) o0[e] = o[e] = bf16_f(syn1[(int64_t)t * P + e]);
+          for (int j = 0; j < n; j++) {
+            float* v = cur + (int64_t)ctx[j] * d;
+            float x = dot_f32(cfg, v, o);
+            float g = grad_f32(cfg, x, k == 0, alphas[s]);
+            for (int e = 0; e < d; e++) {
+              float vo = v[e];
+              v[e] = fmaf(g, o[e], vo);
+              o[e] = fmaf(g, vo, o[e]);
+            }
+          }
+          for (int e = 0; e < d; e++) delta[e] = o[e] - o0[e];
+          bf16_writeback(syn1 + (int64_t)t * P, delta, d, cfg->vec,
+                         sr_event_key(seed, (uint64_t)s, (uint64_t)w * (K + 1) + k), (uint64_t)t);
+        }
+      }
+      if (w - W >= 0) {
+        int p = w - W;
+        for (int e = 0; e < d; e++) delta[e] = cur[(int64_t)p * d + e] - orig[(int64_t)p * d + e];
+        bf16_writeback(syn0 + (int64_t)sid[p] * P, delta, d, cfg->vec,
+                       sr_event_key(seed, (uint64_t)s, (uint64_t)L * (K + 1) + p), (uint64_t)sid[p]);
+      }
+      if (w + W + 1 < L) {
+        int p = w + W + 1;
+        for (int e = 0; e < d; e++) cur[(int64_t)p * d + e] = orig[(int64_t)p * d + e] = bf16_f(syn0[(int64_t)sid[p] * P + e]);
+      }
+    }
+    for (int p = L - W > 0 ? L - W : 0; p < L; p++) {
+      for (int e = 0; e < d; e++) delta[e] = cur[(int64_t)p * d + e] - orig[(int64_t)p * d + e];
+      bf16_writeback(syn0 + (int64_t)sid[p] * P, delta, d, cfg->vec,
+                     sr_event_key(seed, (uint64_t)s, (uint64_t)L * (K + 1) + p), (uint64_t)sid[p]);
+    }
+  }
+  free(cur);
+  free(orig);
+  free(o);
+  free(o0);
+  free(delta);
+  free(ctx);
+  return rc;
+}
+
 static double log_sigmoid(double x) {
   return x >= 0 ? -log1p(exp(-x)) : x - log1p(exp(x));
 }

@@ -119,6 +119,16 @@ int orc_train_f64(const orc_train_cfg* cfg, double* syn0, double* syn1neg, int64
                   int64_t n_sent, const int64_t* starts, const int32_t* lens, const float* alphas,
                   const int32_t* ids, const int32_t* negs);
 
+/* The same on bfloat16 tables (uint16 bit patterns): loads widen exactly, math
+ * is the FP32 mode's, every write-back is row = SR(row + delta) with the
+ * library's counter-based bits: seed of the training launch, sentence s as
+ * uid, target k of centre w as event w*(K+1)+k, leaving position q as event
+ * L*(K+1)+q; 16 bits per element from the element's vector (cfg->vec wide). */
+int orc_train_bf16(const orc_train_cfg* cfg, uint16_t* syn0, uint16_t* syn1neg, int64_t V, int64_t n_sent,
+                   const int64_t* starts, const int32_t* lens, const float* alphas, const int32_t* ids,
+                   const int32_t* negs, uint64_t seed);
+uint16_t orc_bf16_nearest(float x);
+
 /* Held-out SGNS loss in FP64: for every centre w and context c of every
  * sentence, -log sigma(<v_c, o_w>) - sum_k log sigma(-<v_c, o_nk>), negatives
  * given per centre.  Returns the sum; *pairs gets the number of (c, w) pairs. */

@@ -79,6 +79,11 @@ def _declare(L):
         f = getattr(L, name)
         f.restype = C.c_int
         f.argtypes = [C.POINTER(TrainCfg), P, P, C.c_int64, C.c_int64, P, P, P, P, P]
+    L.orc_train_bf16.restype = C.c_int
+    L.orc_train_bf16.argtypes = [C.POINTER(TrainCfg), P, P, C.c_int64, C.c_int64, P, P, P, P, P,
+                                 C.c_uint64]
+    L.orc_bf16_nearest.restype = C.c_uint16
+    L.orc_bf16_nearest.argtypes = [C.c_float]
     L.orc_cpu_sgns.restype = C.c_int
     L.orc_cpu_sgns.argtypes = [C.POINTER(SamplerCfg), C.POINTER(TrainCfg), P, P, C.c_int,
                                C.c_int64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
@@ -251,6 +256,44 @@ def train(syn0, syn1neg, lens, alphas, ids, negs, *, d, window, negative, sigmoi
             _p(lens), _p(alphas), _p(ids), _p(negs))
     if rc != 0:
         raise RuntimeError(f"oracle train failed: {rc}")
+
+
+def mix64(z: int) -> int:
+    M = (1 << 64) - 1
+    z = (z + 0x9E3779B97F4A7C15) & M
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M
+    return z ^ (z >> 31)
+
+
+def bf16_bits(x: np.ndarray) -> np.ndarray:
+    """float32 -> bfloat16 bit patterns, round to nearest even."""
+    b = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    return ((b + 0x7FFF + ((b >> 16) & 1)) >> 16).astype(np.uint16)
+
+
+def bf16_float(h: np.ndarray) -> np.ndarray:
+    return (h.astype(np.uint32) << 16).view(np.float32)
+
+
+def train_bf16(syn0, syn1neg, lens, alphas, ids, negs, *, d, window, negative, seed, sigmoid="table",
+               vec=4, nv=1):
+    """Serial SGNS on bfloat16 tables (uint16 arrays, updated in place) with the
+    library's stochastic rounding (seed = the training launch's seed)."""
+    table = exp_table()
+    cfg = _train_cfg(d, syn0.shape[1], window, negative, 0 if sigmoid == "table" else 1, vec, nv, table)
+    lens = np.ascontiguousarray(lens, np.int32)
+    starts = np.zeros(len(lens), np.int64)
+    if len(lens) > 1:
+        starts[1:] = np.cumsum(lens[:-1].astype(np.int64))
+    alphas = np.ascontiguousarray(alphas, np.float32)
+    ids = np.ascontiguousarray(ids, np.int32)
+    negs = np.ascontiguousarray(negs, np.int32) if negs.size else np.zeros(1, np.int32)
+    assert syn0.dtype == np.uint16 and syn1neg.dtype == np.uint16
+    rc = lib().orc_train_bf16(C.byref(cfg), _p(syn0), _p(syn1neg), syn0.shape[0], len(lens),
+                              _p(starts), _p(lens), _p(alphas), _p(ids), _p(negs), seed)
+    if rc != 0:
+        raise RuntimeError(f"oracle bf16 train failed: {rc}")
 
 
 def heldout_loss(syn0, syn1neg, lens, ids, negs, *, d, window, negative):

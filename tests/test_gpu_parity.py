@@ -296,3 +296,85 @@ def test_out_of_range_ids_are_rejected_and_handle_survives():
         assert e.value.status == 5
         t.train_sentences([3], [0.02], np.array([1, 2, 3], np.int32), np.ones(6, np.int32))
         assert np.isfinite(t.syn0()).all()
+
+
+# ---------------------------------------------------------------------------
+# bfloat16 tables: FP32 math, stochastic-rounded write-back
+# ---------------------------------------------------------------------------
+
+def _first_launch_seed():
+    # The library seeds the rounding of its n-th training launch with
+    # mix64(0x5EEDF00D + n); a fresh handle's first epoch is launch 0.
+    return O.mix64(0x5EEDF00D)
+
+
+@pytest.mark.parametrize("name,d", [("zipf_t1", 128), ("eos_t1", 100), ("zipf_t3", 300), ("k0_t1", 64)])
+def test_deterministic_bf16_epoch_bit_exact(name, d):
+    """Same sampler, FP32 math in the kernel's order, and the same counter-based
+    stochastic rounding as the oracle: the tables agree bit for bit."""
+    g = load(name)
+    c = dict(g["cfg"])
+    c["iter"] = 1
+    corpus = corpus_of(g)
+    vec, nv, pitch = fw2v.lane_layout(d)
+    with trainer_for(corpus, c, layer_size=d, deterministic=1, precision=fw2v.BF16) as t:
+        s0 = O.bf16_bits(t.syn0())
+        s1 = np.zeros_like(s0)
+        t.train_epoch()
+        got0, got1 = O.bf16_bits(t.syn0()), O.bf16_bits(t.syn1neg())
+    # every batch entry in stream order (zero-length ones too): the kernel's sentence numbers
+    lens, alphas, ids, negs = _flatten_epoch(_oracle_epoch(corpus, c), 0)
+    O.train_bf16(s0, s1, lens, alphas, ids, negs, d=d, window=c["window"], negative=c["negative"],
+                 seed=_first_launch_seed(), vec=vec, nv=nv)
+    np.testing.assert_array_equal(got0, s0)
+    np.testing.assert_array_equal(got1, s1)
+    assert got1.any()
+
+
+def test_bf16_per_step_error_within_one_ulp_of_fp64():
+    """Stated bound for the bfloat16 form: from the GPU's own state, one
+    sentence's update lands within one bfloat16 ulp of the FP64 update of the
+    same state (stochastic rounding picks one of the two neighbours)."""
+    g = load("zipf_t1")
+    c = dict(g["cfg"])
+    c["iter"] = 1
+    corpus = corpus_of(g)
+    d = 128
+    lens, alphas, ids, negs = _flatten_epoch(_oracle_epoch(corpus, c), 0)
+    starts = np.concatenate([[0], np.cumsum(lens[:-1])]).astype(np.int64)
+    K = c["negative"]
+    with trainer_for(corpus, c, layer_size=d, deterministic=1, sigmoid=fw2v.SIGMOID_EXACT,
+                     precision=fw2v.BF16) as t:
+        rng = np.random.default_rng(5)
+        t.set_tables(None, (rng.standard_normal((len(corpus.counts), d)) * 0.05).astype(np.float32))
+        worst = 0.0
+        for s in [i for i in range(len(lens)) if lens[i] > 0][:8]:
+            a0, a1 = t.syn0(), t.syn1neg()
+            sl = slice(starts[s], starts[s] + lens[s])
+            sid, sneg = ids[sl], negs[starts[s] * K:(starts[s] + lens[s]) * K]
+            t.train_sentences([lens[s]], [alphas[s]], sid, sneg)
+            b0, b1 = t.syn0(), t.syn1neg()
+            r0, r1 = a0.astype(np.float64), a1.astype(np.float64)
+            O.train(r0, r1, [lens[s]], [alphas[s]], sid, sneg, d=d, window=c["window"], negative=K,
+                    sigmoid="exact", precision=64)
+            for got, ref in ((b0, r0), (b1, r1)):
+                mag = np.maximum(np.abs(ref), 1e-30)
+                ulp = 2.0 ** (np.floor(np.log2(mag)) - 7)
+                worst = max(worst, float((np.abs(got.astype(np.float64) - ref) / ulp).max()))
+        assert worst <= 1.001, worst
+
+
+def test_bf16_hogwild_learns_like_fp32():
+    g = load("zipf_t1")
+    c = dict(g["cfg"])
+    corpus = corpus_of(g)
+    lens, alphas, ids, negs = _flatten_epoch(_oracle_epoch(corpus, dict(c, iter=1)), 0)
+    losses = {}
+    for prec in (fw2v.FP32, fw2v.BF16):
+        with trainer_for(corpus, c, layer_size=64, precision=prec) as t:
+            before, _ = t.heldout_loss(lens, ids, negs)
+            assert t.train() == int(g["overall_words"])
+            after, _ = t.heldout_loss(lens, ids, negs)
+            assert np.isfinite(t.syn0()).all() and after < before
+            losses[prec] = after
+    assert abs(losses[fw2v.BF16] - losses[fw2v.FP32]) <= 0.02 * losses[fw2v.FP32]
