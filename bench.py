@@ -393,7 +393,7 @@ def synth_text(args, cfg):
     from fw2v import synth
     n = args.tokens or cfg["n_tokens"]
     seed = 1234 + int(args.config[1:])
-    raw, _ = synth.topic_tokens(n, cfg["vocab"], cfg["topics"], cfg["zipf_s"], seed=seed)
+    raw, _, _ = synth.topic_tokens(n, cfg["vocab"], cfg["topics"], cfg["zipf_s"], seed=seed)
     ends = np.arange(1000, len(raw) + 1000, 1000)
     ends[-1] = len(raw)
     tmp = tempfile.mkdtemp(prefix="fw2v_ref_")

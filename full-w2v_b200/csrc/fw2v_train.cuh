@@ -263,11 +263,22 @@ __device__ __forceinline__ void row_load_global(Row<VEC, NV>& r, const bf16_t* r
   }
 }
 
-// row = SR(row + (a - b)) per element, 16 random bits each from the event key:
-// a compare-and-swap loop per vector (64-bit for 4 elements, 32-bit for 2,
-// 16-bit per element of a vector straddling d).  Lost races retry with the
-// current value; after 64 failed attempts the update is dropped (a Hogwild
-// lost update) so that the loop always ends.
+// bfloat16 write-back of a row that moved from b (its value when loaded) to a
+// (FP32): s = the stochastic rounding of a (bf16_stochastic, 16 random bits
+// per element from the event key), and the increment s - b, rounded to
+// bfloat16, is added to the stored row with the hardware's fire-and-forget
+// bfloat16 reduction (red.add.noftz: exact sum rounded to nearest even,
+// subnormals kept).  s - b is a multiple of the finer of the two values' ulps,
+// so it is exact in bfloat16 unless the change exceeds 255 of them; then, when
+// no other writer touched the row since the load, the stored value becomes s
+// exactly.  Concurrent writers never lose each other's updates.
+__device__ __forceinline__ uint32_t sr_increment2(float a0, float b0, float a1, float b1, uint32_t r32) {
+  const float x0 = __fsub_rn(bf16_value(bf16_stochastic(a0, r32 & 0xFFFFu)), b0);
+  const float x1 = __fsub_rn(bf16_value(bf16_stochastic(a1, r32 >> 16)), b1);
+  const __nv_bfloat162 v = __floats2bfloat162_rn(x0, x1);  // x0 in the low half (lower address)
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+
 template <int VEC, int NV>
 __device__ __forceinline__ void row_add_delta(bf16_t* row, const Row<VEC, NV>& a, const Row<VEC, NV>& b, int lane,
                                               int d, uint64_t key, uint64_t row_id) {
@@ -277,51 +288,23 @@ __device__ __forceinline__ void row_add_delta(bf16_t* row, const Row<VEC, NV>& a
     const int e = (i * 32 + lane) * VEC;
     if (e >= d) continue;
     const uint64_t bits = sr_vector_bits(key, row_id, (uint64_t)(e / VEC));
-    float dl[VEC];
-#pragma unroll
-    for (int j = 0; j < VEC; j++) dl[j] = __fsub_rn(a.x[i][j], b.x[i][j]);
     if (e + VEC <= d) {
+      const uint32_t p0 = sr_increment2(a.x[i][0], b.x[i][0], a.x[i][1], b.x[i][1], (uint32_t)bits);
       if constexpr (VEC == 4) {
-        unsigned long long* addr = reinterpret_cast<unsigned long long*>(h + e);
-        unsigned long long old = __ldcg(addr);
-        for (int it = 0; it < 64; it++) {
-          unsigned long long nv = 0;
-#pragma unroll
-          for (int j = 0; j < 4; j++) {
-            const float cur = bf16_value((uint16_t)(old >> (16 * j)));
-            nv |= (unsigned long long)bf16_stochastic(__fadd_rn(cur, dl[j]), (uint32_t)(bits >> (16 * j))) << (16 * j);
-          }
-          const unsigned long long prev = atomicCAS(addr, old, nv);
-          if (prev == old) break;
-          old = prev;
-        }
+        const uint32_t p1 = sr_increment2(a.x[i][2], b.x[i][2], a.x[i][3], b.x[i][3], (uint32_t)(bits >> 32));
+        asm volatile("red.global.add.noftz.v2.bf16x2 [%0], {%1, %2};" ::"l"(h + e), "r"(p0), "r"(p1) : "memory");
       } else {
-        unsigned* addr = reinterpret_cast<unsigned*>(h + e);
-        unsigned old = __ldcg(addr);
-        for (int it = 0; it < 64; it++) {
-          unsigned nv = 0;
-#pragma unroll
-          for (int j = 0; j < 2; j++) {
-            const float cur = bf16_value((uint16_t)(old >> (16 * j)));
-            nv |= (unsigned)bf16_stochastic(__fadd_rn(cur, dl[j]), (uint32_t)(bits >> (16 * j))) << (16 * j);
-          }
-          const unsigned prev = atomicCAS(addr, old, nv);
-          if (prev == old) break;
-          old = prev;
-        }
+        asm volatile("red.global.add.noftz.bf16x2 [%0], %1;" ::"l"(h + e), "r"(p0) : "memory");
       }
     } else {
 #pragma unroll
       for (int j = 0; j < VEC; j++) {
         if (e + j >= d) continue;
-        unsigned short* addr = reinterpret_cast<unsigned short*>(h + e + j);
-        unsigned short old = __ldcg(addr);
-        for (int it = 0; it < 64; it++) {
-          const unsigned short nv = bf16_stochastic(__fadd_rn(bf16_value(old), dl[j]), (uint32_t)(bits >> (16 * j)));
-          const unsigned short prev = atomicCAS(addr, old, nv);
-          if (prev == old) break;
-          old = prev;
-        }
+        const uint32_t r16 = (uint32_t)(bits >> (16 * j)) & 0xFFFFu;
+        const float x = __fsub_rn(bf16_value(bf16_stochastic(a.x[i][j], r16)), b.x[i][j]);
+        const __nv_bfloat16 v = __float2bfloat16_rn(x);
+        const unsigned short u = *reinterpret_cast<const unsigned short*>(&v);
+        asm volatile("red.global.add.noftz.bf16 [%0], %1;" ::"l"(h + e + j), "h"(u) : "memory");
       }
     }
   }

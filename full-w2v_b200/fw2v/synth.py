@@ -24,6 +24,9 @@ class SynthCorpus:
     chunk_off: np.ndarray    # int64
     label: np.ndarray        # planted topic/block per vocab id (-1 for </s>)
     raw_of_vocab: np.ndarray  # raw id per vocab id (-1 for </s>)
+    # share of a word's expected count that its planted topic contributes
+    # (1 for graph nodes); words above 1/2 carry a recoverable planted label
+    purity: np.ndarray | None = None
 
 
 def topic_tokens(n_tokens: int, vocab: int, topics: int, zipf_s: float, *, sentence_len: int = 1000,
@@ -58,7 +61,9 @@ def topic_tokens(n_tokens: int, vocab: int, topics: int, zipf_s: float, *, sente
     ranks = np.empty((topics, vocab), np.int32)
     ranks[np.arange(topics)[:, None], perm] = np.arange(vocab)[None, :]
     planted = np.argmin(ranks, axis=0).astype(np.int32)
-    return out[:n_tokens], planted
+    p = (ranks + 1.0) ** -zipf_s
+    purity = p.max(0) / p.sum(0)
+    return out[:n_tokens], planted, purity
 
 
 def sbm_walks(nodes: int, blocks: int, degree: float, p_ratio: float, walks_per_node: int,
@@ -129,18 +134,12 @@ def build_stream(raw: np.ndarray, sentence_ends: np.ndarray, raw_label: np.ndarr
     vocab_of_raw[order] = np.arange(1, len(order) + 1)
     vid = vocab_of_raw[raw]
     if cache_eos:
-        line = np.zeros(len(raw), np.int64)
-        line[sentence_ends[:-1]] = 1
-        line = np.cumsum(line)
-        keep = vid >= 0
-        toks, pos = [], 0
         parts = []
         bounds = np.concatenate([[0], sentence_ends])
         for i in range(n_lines):
             seg = vid[bounds[i]:bounds[i + 1]]
             parts.append(seg[seg >= 0])
             parts.append(np.zeros(1, np.int64))
-        del toks, pos, keep, line
         ids = np.concatenate(parts).astype(np.int32)
         # chunk at EOS or msl (improved_driver_functions.cpp:270)
         offs, n = [], 0
@@ -190,9 +189,120 @@ def make_topic_corpus(name: str, *, n_tokens: int | None = None, seed: int | Non
     if n_tokens is not None:
         cfg["n_tokens"] = n_tokens
     seed = 1234 + int(name[1:]) if seed is None else seed
-    raw, planted = topic_tokens(cfg["n_tokens"], cfg["vocab"], cfg["topics"], cfg["zipf_s"],
-                                seed=seed)
+    raw, planted, purity = topic_tokens(cfg["n_tokens"], cfg["vocab"], cfg["topics"], cfg["zipf_s"],
+                                        seed=seed)
     ends = np.arange(1000, len(raw) + 1000, 1000)
     ends[-1] = len(raw)
     corpus = build_stream(raw, ends, planted, min_count=cfg["min_count"], msl=msl)
+    corpus.purity = np.concatenate([[0.0], purity[corpus.raw_of_vocab[1:]]])
     return corpus, cfg
+
+
+# ---------------------------------------------------------------------------
+# Device-side generation for the large configurations (seeded torch RNG on the
+# GPU; the same seed gives the same corpus on the same device and software).
+# ---------------------------------------------------------------------------
+
+def _affine_perms(vocab: int, topics: int, rng: np.random.Generator):
+    """Per-topic permutations r -> (a*r + b) mod V with gcd(a, V) = 1."""
+    a, b = [], []
+    while len(a) < topics:
+        x = int(rng.integers(1, vocab))
+        if np.gcd(x, vocab) == 1:
+            a.append(x)
+            b.append(int(rng.integers(0, vocab)))
+    return np.array(a, np.int64), np.array(b, np.int64)
+
+
+def topic_corpus_gpu(n_tokens: int, vocab: int, topics: int, zipf_s: float, *, min_count: int,
+                     msl: int = 1000, sentence_len: int = 1000, dirichlet: float = 0.1, seed: int = 0,
+                     device="cuda", heldout_tokens: int = 0):
+    """The topic-mixture corpus of topic_tokens(), generated with torch on a
+    device (each topic's Zipf law runs over an affine permutation of the
+    vocabulary instead of a random one, so no V x topics table is needed).
+
+    Returns (SynthCorpus, held-out stream as int32 vocab ids or None); the
+    held-out tokens continue the same generator after the training tokens and
+    drop words outside the training vocabulary.
+    """
+    import torch
+
+    rng = np.random.default_rng(seed)
+    a, b = _affine_perms(vocab, topics, rng)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    dev = torch.device(device)
+    cdf = torch.cumsum(torch.arange(1, vocab + 1, device=dev, dtype=torch.float64).pow(-zipf_s), 0)
+    cdf = cdf / cdf[-1]
+    ta = torch.from_numpy(a).to(dev)
+    tb = torch.from_numpy(b).to(dev)
+    total = n_tokens + heldout_tokens
+    n_sent = (total + sentence_len - 1) // sentence_len
+    raw = torch.empty(n_sent * sentence_len, dtype=torch.int32, device=dev)
+    conc = torch.full((topics,), dirichlet, device=dev)
+    chunk = max(1, (1 << 27) // (topics * 4))
+    for s0 in range(0, n_sent, chunk):
+        s1 = min(n_sent, s0 + chunk)
+        g = torch._standard_gamma(conc.expand(s1 - s0, topics).contiguous(), generator=gen)
+        theta = g / g.sum(1, keepdim=True).clamp_min(1e-30)
+        z = torch.multinomial(theta, sentence_len, replacement=True, generator=gen)
+        u = torch.rand((s1 - s0, sentence_len), device=dev, generator=gen, dtype=torch.float64)
+        r = torch.searchsorted(cdf, u).clamp_(max=vocab - 1)
+        raw[s0 * sentence_len:s1 * sentence_len] = ((ta[z] * r + tb[z]) % vocab).reshape(-1).to(torch.int32)
+    raw = raw[:total]
+    # planted topic: the one under which a word's rank (a_z^-1 (w - b_z) mod V) is lowest
+    inv = torch.from_numpy(np.array([pow(int(x), -1, vocab) for x in a], np.int64)).to(dev)
+    words = torch.arange(vocab, device=dev, dtype=torch.int64)
+    best = torch.full((vocab,), vocab, device=dev, dtype=torch.int64)
+    planted = torch.zeros(vocab, device=dev, dtype=torch.int64)
+    psum = torch.zeros(vocab, device=dev, dtype=torch.float64)
+    for zt in range(topics):
+        rk = (inv[zt] * ((words - tb[zt]) % vocab)) % vocab
+        better = rk < best
+        best = torch.where(better, rk, best)
+        planted = torch.where(better, torch.full_like(planted, zt), planted)
+        psum += (rk + 1.0).pow(-zipf_s)
+    purity_raw = (best + 1.0).pow(-zipf_s) / psum
+    train_raw = raw[:n_tokens].long()
+    # vocabulary: count descending, ties by first occurrence, min-count cut
+    cnt = torch.bincount(train_raw, minlength=vocab)
+    first = torch.full((vocab,), n_tokens, device=dev, dtype=torch.int64)
+    first.scatter_reduce_(0, train_raw, torch.arange(n_tokens, device=dev, dtype=torch.int64), reduce="amin")
+    seen = torch.nonzero(cnt).flatten()
+    order = seen[torch.argsort(first[seen], stable=True)]
+    order = order[torch.argsort(-cnt[order], stable=True)]
+    order = order[cnt[order] >= min_count]
+    n_lines = (n_tokens + sentence_len - 1) // sentence_len
+    counts = torch.cat([torch.tensor([max(n_lines - 1, 0)], device=dev), cnt[order]])
+    vocab_of_raw = torch.full((vocab,), -1, device=dev, dtype=torch.int64)
+    vocab_of_raw[order] = torch.arange(1, len(order) + 1, device=dev)
+    vid = vocab_of_raw[train_raw]
+    ids = vid[vid >= 0].to(torch.int32)
+    stream = torch.cat([ids, torch.zeros(1, dtype=torch.int32, device=dev)]).cpu().numpy()
+    chunk_off = np.arange(0, len(ids), msl, dtype=np.int64)
+    counts_np = counts.cpu().numpy().astype(np.uint32)
+    label = np.concatenate([[-1], planted[order].cpu().numpy()]).astype(np.int32)
+    raw_of_vocab = np.concatenate([[-1], order.cpu().numpy()]).astype(np.int64)
+    purity = np.concatenate([[0.0], purity_raw[order].cpu().numpy()])
+    corpus = SynthCorpus(counts_np, int(counts_np.sum()) + 1, stream, chunk_off, label, raw_of_vocab, purity)
+    held = None
+    if heldout_tokens:
+        hv = vocab_of_raw[raw[n_tokens:].long()]
+        held = hv[hv >= 0].to(torch.int32).cpu().numpy()
+    del raw, train_raw, vid, ids
+    if dev.type == "cuda":
+        torch.cuda.empty_cache()
+    return corpus, held
+
+
+def make_topic_corpus_gpu(name: str, *, n_tokens: int | None = None, heldout_tokens: int = 0,
+                          msl: int = 1000, device="cuda"):
+    """A named configuration's topic corpus from topic_corpus_gpu:
+    (corpus, held-out stream, config)."""
+    cfg = dict(CONFIGS[name])
+    if n_tokens is not None:
+        cfg["n_tokens"] = n_tokens
+    corpus, held = topic_corpus_gpu(cfg["n_tokens"], cfg["vocab"], cfg["topics"], cfg["zipf_s"],
+                                    min_count=cfg["min_count"], msl=msl, seed=1234 + int(name[1:]),
+                                    device=device, heldout_tokens=heldout_tokens)
+    return corpus, held, cfg

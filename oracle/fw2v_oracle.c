@@ -397,12 +397,20 @@ uint16_t orc_bf16_nearest(float x) {
   return (uint16_t)((b + 0x7FFFu + ((b >> 16) & 1u)) >> 16);
 }
 
-/* row = SR(row + delta) with the kernel's random bits for (key, row id). */
-static void bf16_writeback(uint16_t* row, const float* delta, int d, int vec, uint64_t key, uint64_t row_id) {
+/* One element of the write-back of a row that moved from b to a: the
+ * increment SR(a) - b, rounded to bfloat16, added to the stored value with
+ * round-to-nearest-even.  Both addends are bfloat16, so their float sum rounds
+ * to the same bfloat16 as the exact sum. */
+uint16_t orc_bf16_writeback1(uint16_t stored, float a, float b, uint32_t r16) {
+  float inc = bf16_f(orc_bf16_nearest(bf16_f(bf16_sr(a, r16)) - b));
+  return orc_bf16_nearest(bf16_f(stored) + inc);
+}
+
+static void bf16_writeback(uint16_t* row, const float* a, const float* b, int d, int vec, uint64_t key,
+                           uint64_t row_id) {
   for (int e = 0; e < d; e++) {
     uint64_t bits = sr_vector_bits(key, row_id, (uint64_t)(e / vec));
-    uint32_t r16 = (uint32_t)(bits >> (16 * (e % vec)));
-    row[e] = bf16_sr(bf16_f(row[e]) + delta[e], r16);
+    row[e] = orc_bf16_writeback1(row[e], a[e], b[e], (uint32_t)(bits >> (16 * (e % vec))) & 0xFFFFu);
   }
 }
 
@@ -421,7 +429,6 @@ int orc_train_bf16(const orc_train_cfg* cfg, uint16_t* syn0, uint16_t* syn1, int
   float* orig = (float*)malloc(sizeof(float) * ((size_t)maxL + 1) * d);
   float* o = (float*)malloc(sizeof(float) * d);
   float* o0 = (float*)malloc(sizeof(float) * d);
-  float* delta = (float*)malloc(sizeof(float) * d);
   int* ctx = (int*)malloc(sizeof(int) * (2 * W + 1));
   int rc = 0;
   for (int64_t s = 0; s < n_sent && rc == 0; s++) {
@@ -453,15 +460,13 @@ int orc_train_bf16(const orc_train_cfg* cfg, uint16_t* syn0, uint16_t* syn1, int
               o[e] = fmaf(g, vo, o[e]);
             }
           }
-          for (int e = 0; e < d; e++) delta[e] = o[e] - o0[e];
-          bf16_writeback(syn1 + (int64_t)t * P, delta, d, cfg->vec,
+          bf16_writeback(syn1 + (int64_t)t * P, o, o0, d, cfg->vec,
                          sr_event_key(seed, (uint64_t)s, (uint64_t)w * (K + 1) + k), (uint64_t)t);
         }
       }
       if (w - W >= 0) {
         int p = w - W;
-        for (int e = 0; e < d; e++) delta[e] = cur[(int64_t)p * d + e] - orig[(int64_t)p * d + e];
-        bf16_writeback(syn0 + (int64_t)sid[p] * P, delta, d, cfg->vec,
+        bf16_writeback(syn0 + (int64_t)sid[p] * P, cur + (int64_t)p * d, orig + (int64_t)p * d, d, cfg->vec,
                        sr_event_key(seed, (uint64_t)s, (uint64_t)L * (K + 1) + p), (uint64_t)sid[p]);
       }
       if (w + W + 1 < L) {
@@ -470,8 +475,7 @@ int orc_train_bf16(const orc_train_cfg* cfg, uint16_t* syn0, uint16_t* syn1, int
       }
     }
     for (int p = L - W > 0 ? L - W : 0; p < L; p++) {
-      for (int e = 0; e < d; e++) delta[e] = cur[(int64_t)p * d + e] - orig[(int64_t)p * d + e];
-      bf16_writeback(syn0 + (int64_t)sid[p] * P, delta, d, cfg->vec,
+      bf16_writeback(syn0 + (int64_t)sid[p] * P, cur + (int64_t)p * d, orig + (int64_t)p * d, d, cfg->vec,
                      sr_event_key(seed, (uint64_t)s, (uint64_t)L * (K + 1) + p), (uint64_t)sid[p]);
     }
   }
@@ -479,7 +483,6 @@ int orc_train_bf16(const orc_train_cfg* cfg, uint16_t* syn0, uint16_t* syn1, int
   free(orig);
   free(o);
   free(o0);
-  free(delta);
   free(ctx);
   return rc;
 }

@@ -128,6 +128,10 @@ int orc_train_bf16(const orc_train_cfg* cfg, uint16_t* syn0, uint16_t* syn1neg, 
                    const int64_t* starts, const int32_t* lens, const float* alphas, const int32_t* ids,
                    const int32_t* negs, uint64_t seed);
 uint16_t orc_bf16_nearest(float x);
+/* One element of the bfloat16 write-back: `stored` after its row moved from b
+ * to a, with 16 random bits r16 (increment to the stochastic rounding of a,
+ * added with round-to-nearest). */
+uint16_t orc_bf16_writeback1(uint16_t stored, float a, float b, uint32_t r16);
 
 /* Held-out SGNS loss in FP64: for every centre w and context c of every
  * sentence, -log sigma(<v_c, o_w>) - sum_k log sigma(-<v_c, o_nk>), negatives

@@ -84,6 +84,8 @@ def _declare(L):
                                  C.c_uint64]
     L.orc_bf16_nearest.restype = C.c_uint16
     L.orc_bf16_nearest.argtypes = [C.c_float]
+    L.orc_bf16_writeback1.restype = C.c_uint16
+    L.orc_bf16_writeback1.argtypes = [C.c_uint16, C.c_float, C.c_float, C.c_uint32]
     L.orc_cpu_sgns.restype = C.c_int
     L.orc_cpu_sgns.argtypes = [C.POINTER(SamplerCfg), C.POINTER(TrainCfg), P, P, C.c_int,
                                C.c_int64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
@@ -274,6 +276,12 @@ def bf16_bits(x: np.ndarray) -> np.ndarray:
 
 def bf16_float(h: np.ndarray) -> np.ndarray:
     return (h.astype(np.uint32) << 16).view(np.float32)
+
+
+def bf16_writeback1(stored: int, a: float, b: float, r16: int) -> int:
+    """One element of the bfloat16 write-back: the stored bits after the row
+    moved from b to a, with 16 random bits."""
+    return int(lib().orc_bf16_writeback1(stored, a, b, r16))
 
 
 def train_bf16(syn0, syn1neg, lens, alphas, ids, negs, *, d, window, negative, seed, sigmoid="table",
