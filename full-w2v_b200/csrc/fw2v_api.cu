@@ -21,7 +21,8 @@ cudaError_t launch_train(const TrainParams& p, int num_sms, cudaStream_t st);
 cudaError_t launch_heldout(const TrainParams& p, double* loss, unsigned long long* pairs, cudaStream_t st);
 cudaError_t launch_init_tables(void* syn0, bool bf16, int64_t V, int d, int64_t pitch, const uint32_t* d_counts,
                                float sample, uint64_t train_words, int32_t* keep_thr, const int64_t* d_firsts,
-                               int n_firsts, int32_t* unigram, int64_t table_size, cudaStream_t st);
+                               int n_firsts, int32_t* unigram, int64_t table_size, uint64_t start,
+                               cudaStream_t st);
 size_t train_smem_bytes(int window, int64_t pitch, int warps, int r);
 int64_t train_scratch_warps(int num_sms);
 cudaError_t launch_validate_ids(const int32_t* ids, int64_t n, int64_t vocab, int* flag, cudaStream_t st);
@@ -168,7 +169,7 @@ TrainParams base_train_params(fw2v_handle* h) {
   p.orig_scratch = h->orig_scratch;
   p.scratch_warps = h->scratch_warps;
   p.bf16 = h->cfg.precision == FW2V_BF16;
-  p.sr_seed = mix64(0x5EEDF00DULL + h->launches);
+  p.sr_seed = mix64(0x5EEDF00DULL + h->launches + seed_offset(h->cfg.seed));
   return p;
 }
 
@@ -335,7 +336,7 @@ fw2v_status fw2v_set_vocab(fw2v_handle* h, const uint32_t* counts, int64_t V, ui
   CK(h, cudaMemcpyAsync(d_counts, counts, V * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaMemcpyAsync(d_firsts, firsts.data(), (V - 1) * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
   CK(h, launch_init_tables(h->syn0, h->elem == 2, V, d, P, d_counts, h->cfg.sample, train_words, h->keep_thr, d_firsts,
-                           (int)(V - 1), h->unigram, kUnigramTableSize, h->stream));
+                           (int)(V - 1), h->unigram, kUnigramTableSize, 1ULL + seed_offset(h->cfg.seed), h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
   dfree(d_counts);
   dfree(d_firsts);
@@ -424,7 +425,7 @@ fw2v_status fw2v_load_corpus(fw2v_handle* h, const int32_t* stream, int64_t stre
   // Stream state (FULL-W2V-driver.cu:113-114): LCG seeded with the id, alpha0.
   std::vector<uint64_t> lcg(T), zero(T, 0);
   std::vector<float> alpha(T, h->cfg.alpha);
-  for (int i = 0; i < T; i++) lcg[i] = (uint64_t)i;
+  for (int i = 0; i < T; i++) lcg[i] = (uint64_t)i + seed_offset(h->cfg.seed);
   CK(h, cudaMemcpyAsync(h->lcg, lcg.data(), T * sizeof(uint64_t), cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaMemcpyAsync(h->wca, zero.data(), T * sizeof(uint64_t), cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaMemcpyAsync(h->alpha, alpha.data(), T * sizeof(float), cudaMemcpyHostToDevice, h->stream));

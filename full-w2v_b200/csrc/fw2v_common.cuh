@@ -46,6 +46,9 @@ __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
   return z ^ (z >> 31);
 }
+// Offset of every LCG start state and stochastic-rounding seed for a
+// configuration's seed (0 for seed 0: the reference's seeds).
+__host__ __device__ __forceinline__ uint64_t seed_offset(uint64_t seed) { return seed ? mix64(seed) : 0; }
 __host__ __device__ __forceinline__ uint64_t sr_event_key(uint64_t seed, uint64_t uid, uint64_t event) {
   return mix64(seed ^ mix64(uid * 0x9E3779B97F4A7C15ULL + event));
 }
@@ -105,7 +108,9 @@ struct SamplerParams {
   int64_t vocab;
   const int32_t* keep_thr;  // keep a token iff (lcg & 0xFFFF) <= keep_thr[word]
   float sample;
-  const int32_t* unigram;
+  const int32_t* unigram;         // the table, or null: search unigram_firsts
+  const int64_t* unigram_firsts;  // first table index of words 1..n_firsts (non-decreasing)
+  int64_t n_firsts;
   int64_t table_size;
   const uint64_t* jump_a;   // r -> jump_a[m] * r + jump_c[m] is m LCG steps
   const uint64_t* jump_c;
@@ -128,6 +133,20 @@ struct SamplerParams {
   uint64_t* words;
   int* error_flag;
 };
+
+// Unigram table entry `a` (FULL-W2V-driver.cu:224-227): the table itself, or
+// the same value from the run boundaries: the word whose run [firsts[j],
+// firsts[j+1]) holds a is j+1 (the search the table fill uses).
+__device__ __forceinline__ int32_t unigram_pick(const SamplerParams& p, int64_t a) {
+  if (p.unigram) return __ldg(p.unigram + a);
+  int64_t lo = 0, hi = p.n_firsts - 1;  // last j with firsts[j] <= a (firsts[0] == 0)
+  while (lo < hi) {
+    const int64_t mid = (lo + hi + 1) >> 1;
+    if (__ldg(p.unigram_firsts + mid) <= a) lo = mid;
+    else hi = mid - 1;
+  }
+  return (int32_t)(lo + 1);
+}
 
 __host__ __device__ __forceinline__ void stream_range(int64_t n_chunks, int threads, int s,
                                                       int64_t* first, int64_t* end) {
@@ -179,7 +198,33 @@ struct TrainParams {
   int64_t scratch_warps;
   uint64_t sr_seed;  // stochastic rounding of bfloat16 write-backs
   int bf16;          // tables hold bfloat16
+  // batched launches: lane vector width (2 or 4, one vector per lane) and
+  // pipeline stages of this job's sentences
+  int lane_vec, stages;
 };
+
+// A round of a batched epoch: n sampling streams of any jobs.  Stream g of the
+// round is stream local[g] of job job[g], whose carried state is at index
+// gstream[g] of the batch's state arrays; its kept ids start at kbase[g] and
+// its entries at kbase[g] + 2g of the round's buffers (kbase has n + 1 entries).
+struct BatchRound {
+  const int32_t* job;
+  const int32_t* local;
+  const int64_t* gstream;
+  const int64_t* kbase;
+  int n;
+};
+
+// A parameter block copied into shared memory by the lanes t = 0..n-1 of a
+// warp or block, one 32-bit word each, so that per-job parameters read from
+// there in a kernel's inner loops (global stores cannot alias them).
+template <typename P>
+__device__ __forceinline__ void copy_params(P* dst, const P* src, int t, int n) {
+  static_assert(sizeof(P) % 4 == 0, "parameter blocks are word-sized");
+  uint32_t* d = reinterpret_cast<uint32_t*>(dst);
+  const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+  for (int i = t; i < (int)(sizeof(P) / 4); i += n) d[i] = s[i];
+}
 
 // Sampler output layout: stream s keeps its kept ids at [stream_base[s],
 // stream_base[s+1]) and its batch entries from stream_base[s] + 2s (one more

@@ -34,15 +34,13 @@ constexpr uint32_t kLcgAdd32 = (uint32_t)kLcgAdd;
 
 }  // namespace
 
-__global__ void __launch_bounds__(128) sampler_warp_kernel(SamplerParams p) {
-  const int lane = threadIdx.x & 31;
-  const int s = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  if (s >= p.threads) return;
-  int64_t es, ee;
-  stream_range(p.n_chunks, p.threads, s, &es, &ee);
-  const int64_t kept_base = p.stream_base[s];
-  const int64_t kept_cap = p.stream_base[s + 1] - kept_base;
-  const int64_t entry_b = entry_base(p.stream_base, s);
+// One stream's epoch: the chunks [es, ee) of the job's chunk table, kept ids
+// from kept_base (at most kept_cap), entries from entry_b; the stream's
+// carried state is at index `st` of p.lcg / wca_own / alpha, its counts at
+// index `so` of p.n_entries / n_kept / words.
+__device__ __forceinline__ void sample_stream(const SamplerParams& p, int64_t es, int64_t ee, int64_t kept_base,
+                                              int64_t kept_cap, int64_t entry_b, int64_t st, int64_t so,
+                                              int lane) {
   const int64_t entry_cap = kept_cap + 2;
   const int K = p.negative;
   const int msl = p.msl;
@@ -50,10 +48,10 @@ __global__ void __launch_bounds__(128) sampler_warp_kernel(SamplerParams p) {
   const uint32_t aK = (uint32_t)p.jump_a[K];
   const uint32_t cK = (uint32_t)p.jump_c[K];
 
-  uint64_t r_blk = p.lcg[s];  // full state at the start of the current block
+  uint64_t r_blk = p.lcg[st];  // full state at the start of the current block
   uint32_t r32 = (uint32_t)r_blk;
-  uint64_t wca_own = p.wca_own[s];
-  float alpha = p.alpha[s];
+  uint64_t wca_own = p.wca_own[st];
+  float alpha = p.alpha[st];
   uint64_t word_count = 0, last_word_count = 0;
   int64_t nk = 0, ne = 0;
   int L = 0;
@@ -165,29 +163,42 @@ __global__ void __launch_bounds__(128) sampler_warp_kernel(SamplerParams p) {
     nk = 0;
   }
   if (lane == 0) {
-    p.lcg[s] = r_blk;
-    p.wca_own[s] = wca_own;
-    p.alpha[s] = alpha;
-    p.n_entries[s] = ne;
-    p.n_kept[s] = nk;
-    p.words[s] = word_count;
+    p.lcg[st] = r_blk;
+    p.wca_own[st] = wca_own;
+    p.alpha[st] = alpha;
+    p.n_entries[so] = ne;
+    p.n_kept[so] = nk;
+    p.words[so] = word_count;
   }
+}
+
+__global__ void __launch_bounds__(128) sampler_warp_kernel(SamplerParams p) {
+  const int lane = threadIdx.x & 31;
+  const int s = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (s >= p.threads) return;
+  int64_t es, ee;
+  stream_range(p.n_chunks, p.threads, s, &es, &ee);
+  const int64_t kept_base = p.stream_base[s];
+  sample_stream(p, es, ee, kept_base, p.stream_base[s + 1] - kept_base, entry_base(p.stream_base, s), s, s, lane);
 }
 
 // K negatives of every kept token from its LCG state: the reference draws them
 // right after the token's keep decision, one LCG step each, and indexes the
 // unigram table with (state >> 16) % table_size (FULL-W2V-driver.cu:224-227).
-__global__ void __launch_bounds__(256) negatives_kernel(SamplerParams p) {
-  const int s = blockIdx.y;
-  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= p.threads || k >= p.n_kept[s]) return;
-  const int64_t slot = p.stream_base[s] + k;
+__device__ __forceinline__ void draw_negatives(const SamplerParams& p, int64_t slot) {
   uint64_t r = p.kept_state[slot];
   int32_t* out = p.kept_negs + slot * p.negative;
   for (int j = 0; j < p.negative; j++) {
     r = lcg_next(r);
-    out[j] = __ldg(p.unigram + (int64_t)((r >> 16) % (uint64_t)p.table_size));
+    out[j] = unigram_pick(p, (int64_t)((r >> 16) % (uint64_t)p.table_size));
   }
+}
+
+__global__ void __launch_bounds__(256) negatives_kernel(SamplerParams p) {
+  const int s = blockIdx.y;
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= p.threads || k >= p.n_kept[s]) return;
+  draw_negatives(p, p.stream_base[s] + k);
 }
 
 // Exclusive prefix sum of n_entries over streams (one block), so that the
@@ -280,6 +291,81 @@ __global__ void stream_base_kernel(const int64_t* chunk_base, int64_t n_chunks, 
   int64_t first, end;
   stream_range(n_chunks, threads, s, &first, &end);
   stream_base[s] = chunk_base[first];
+}
+
+// ---- batched jobs: one launch over a round's (job, stream) list ----
+
+// One warp per stream of the round; jobs past their epoch count record nothing.
+__global__ void __launch_bounds__(128) sampler_batch_kernel(const SamplerParams* jobs, BatchRound r, int epoch) {
+  __shared__ __align__(8) SamplerParams sp[4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (g >= r.n) return;
+  copy_params(&sp[warp], &jobs[r.job[g]], lane, 32);
+  __syncwarp();
+  const SamplerParams& p = sp[warp];
+  if (epoch >= p.epochs) {
+    if (lane == 0) {
+      p.n_entries[g] = 0;
+      p.n_kept[g] = 0;
+      p.words[g] = 0;
+    }
+    return;
+  }
+  int64_t es, ee;
+  stream_range(p.n_chunks, p.threads, r.local[g], &es, &ee);
+  const int64_t kb = r.kbase[g];
+  sample_stream(p, es, ee, kb, r.kbase[g + 1] - kb, kb + 2 * g, r.gstream[g], g, lane);
+}
+
+// blockIdx.y = stream of the round.
+__global__ void __launch_bounds__(256) negatives_batch_kernel(const SamplerParams* jobs, BatchRound r) {
+  __shared__ __align__(8) SamplerParams sp;
+  const int g = blockIdx.y;
+  copy_params(&sp, &jobs[r.job[g]], threadIdx.x, blockDim.x);
+  __syncthreads();
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= sp.n_kept[g]) return;
+  draw_negatives(sp, r.kbase[g] + k);
+}
+
+// One thread per job: the number of the job's first sentence in each of its
+// round streams (its sentences are numbered in stream order over the epoch,
+// as a single job's are), and the job's words read and kept.
+__global__ void round_jobs_kernel(BatchRound r, const int64_t* n_entries, const int64_t* n_kept,
+                                  const uint64_t* words, int n_jobs, int64_t* job_uid, int64_t* uid_base,
+                                  unsigned long long* job_words, unsigned long long* job_kept) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n_jobs) return;
+  int64_t run = job_uid[j];
+  unsigned long long w = 0, k = 0;
+  for (int g = 0; g < r.n; g++) {
+    if (r.job[g] != j) continue;
+    uid_base[g] = run;
+    run += n_entries[g];
+    w += words[g];
+    k += (unsigned long long)n_kept[g];
+  }
+  job_uid[j] = run;
+  job_words[j] += w;
+  job_kept[j] += k;
+}
+
+cudaError_t launch_sampler_round(const SamplerParams* d_jobs, const BatchRound& r, int epoch, int64_t max_region,
+                                 bool any_negatives, const int64_t* n_entries, const int64_t* n_kept,
+                                 const uint64_t* words, int n_jobs, int64_t* job_uid, int64_t* uid_base,
+                                 unsigned long long* job_words, unsigned long long* job_kept,
+                                 int64_t* entry_prefix, cudaStream_t st) {
+  if (r.n < 1 || r.n > 65535) return cudaErrorInvalidValue;
+  sampler_batch_kernel<<<(r.n + 3) / 4, 128, 0, st>>>(d_jobs, r, epoch);
+  if (any_negatives && max_region > 0) {
+    const dim3 grid((unsigned)((max_region + 255) / 256), (unsigned)r.n);
+    negatives_batch_kernel<<<grid, 256, 0, st>>>(d_jobs, r);
+  }
+  entry_prefix_kernel<<<1, 1024, 0, st>>>(n_entries, r.n, entry_prefix);
+  round_jobs_kernel<<<(n_jobs + 127) / 128, 128, 0, st>>>(r, n_entries, n_kept, words, n_jobs, job_uid, uid_base,
+                                                        job_words, job_kept);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_corpus_layout(const int32_t* stream, int64_t stream_len, const int64_t* chunk_off,

@@ -18,14 +18,14 @@
 namespace fw2v {
 
 // improved_driver_functions.cpp:27-31; element i = row*d + c uses the
-// (i+1)-th LCG state from seed 1.  One thread per row, started by jump-ahead.
-// Bfloat16 tables take the FP32 value rounded to nearest.
+// (i+1)-th LCG state from `start` (1 in the reference).  One thread per row,
+// started by jump-ahead.  Bfloat16 tables take the FP32 value rounded to nearest.
 template <typename T>
-__global__ void init_syn0_kernel(T* syn0, int64_t V, int d, int64_t pitch) {
+__global__ void init_syn0_kernel(T* syn0, int64_t V, int d, int64_t pitch, uint64_t start) {
   const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (row >= V) return;
   const Affine j = lcg_jump((uint64_t)row * (uint64_t)d);
-  uint64_t r = j.a * 1ULL + j.c;  // state after row*d steps from seed 1
+  uint64_t r = j.a * start + j.c;  // state after row*d steps from `start`
   T* out = syn0 + row * pitch;
   const float fd = (float)d;
   for (int c = 0; c < d; c++) {
@@ -113,12 +113,12 @@ namespace fw2v {
 cudaError_t launch_init_tables(void* syn0, bool bf16, int64_t V, int d, int64_t pitch, const uint32_t* d_counts,
                                float sample, uint64_t train_words, int32_t* keep_thr,
                                const int64_t* d_firsts, int n_firsts, int32_t* unigram,
-                               int64_t table_size, cudaStream_t st) {
+                               int64_t table_size, uint64_t start, cudaStream_t st) {
   const int b = 256;
-  if (bf16) init_syn0_kernel<<<(unsigned)((V + b - 1) / b), b, 0, st>>>((uint16_t*)syn0, V, d, pitch);
-  else init_syn0_kernel<<<(unsigned)((V + b - 1) / b), b, 0, st>>>((float*)syn0, V, d, pitch);
+  if (bf16) init_syn0_kernel<<<(unsigned)((V + b - 1) / b), b, 0, st>>>((uint16_t*)syn0, V, d, pitch, start);
+  else init_syn0_kernel<<<(unsigned)((V + b - 1) / b), b, 0, st>>>((float*)syn0, V, d, pitch, start);
   subsample_kernel<<<(unsigned)((V + b - 1) / b), b, 0, st>>>(d_counts, V, sample, train_words, keep_thr);
-  unigram_fill_kernel<<<148 * 16, 256, 0, st>>>(d_firsts, n_firsts, unigram, table_size);
+  if (unigram) unigram_fill_kernel<<<148 * 16, 256, 0, st>>>(d_firsts, n_firsts, unigram, table_size);
   return cudaGetLastError();
 }
 

@@ -39,12 +39,30 @@ class Config(C.Structure):
         ("epochs", C.c_int32), ("threads", C.c_int32), ("msl", C.c_int32),
         ("alpha", C.c_float), ("sample", C.c_float), ("sigmoid", C.c_int32),
         ("precision", C.c_int32), ("deterministic", C.c_int32), ("device", C.c_int32),
+        ("seed", C.c_uint64),
     ]
 
 
 class EpochStats(C.Structure):
     _fields_ = [("words_read", C.c_uint64), ("words_kept", C.c_uint64),
                 ("sentences", C.c_uint64), ("sampler_ms", C.c_float), ("train_ms", C.c_float)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("device", C.c_int32), ("use_graph", C.c_int32),
+                ("deterministic", C.c_int32), ("round_tokens", C.c_int64)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("words_read", C.c_uint64), ("words_kept", C.c_uint64), ("ms", C.c_float),
+                ("epochs", C.c_int32), ("rounds", C.c_int32)]
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("n_classes", C.c_int32), ("class_d", C.c_int32 * 16), ("class_window", C.c_int32 * 16),
+                ("class_lane_vec", C.c_int32 * 16), ("class_stages", C.c_int32 * 16),
+                ("tuned_wps", C.c_double * 16), ("default_wps", C.c_double * 16),
+                ("warps_per_block", C.c_int32), ("blocks_per_sm", C.c_int32)]
 
 
 # Every entry point declared in include/fw2v.h (tests check the library exports them all).
@@ -56,6 +74,10 @@ EXPORTS = [
     "fw2v_kernel_batch_error", "fw2v_lane_layout", "fw2v_exp_table", "fw2v_unigram_firsts",
     "fw2v_get_unigram", "fw2v_status_string", "fw2v_last_error", "fw2v_version", "fw2v_stream",
     "fw2v_kernel_batch_noalloc", "fw2v_reorder_chunks",
+    "fw2v_batch_config_default", "fw2v_batch_create", "fw2v_batch_destroy", "fw2v_batch_last_error",
+    "fw2v_batch_add_job", "fw2v_batch_set_shape", "fw2v_batch_get_shape", "fw2v_batch_set_launch",
+    "fw2v_batch_get_launch", "fw2v_batch_tune", "fw2v_batch_train", "fw2v_batch_job_words",
+    "fw2v_batch_get_syn0", "fw2v_batch_get_syn1neg",
 ]
 
 _lib = None
@@ -104,6 +126,21 @@ def lib() -> C.CDLL:
             "fw2v_last_error": (C.c_char_p, [H]),
             "fw2v_version": (C.c_char_p, []),
             "fw2v_stream": (C.c_void_p, [H]),
+            "fw2v_batch_config_default": (None, [C.POINTER(BatchConfig)]),
+            "fw2v_batch_create": (C.c_int, [C.POINTER(BatchConfig), C.POINTER(C.c_void_p)]),
+            "fw2v_batch_destroy": (None, [H]),
+            "fw2v_batch_last_error": (C.c_char_p, [H]),
+            "fw2v_batch_add_job": (C.c_int, [H, C.POINTER(Config), P, I64, U64, P, I64, P, I64,
+                                             C.POINTER(I32)]),
+            "fw2v_batch_set_shape": (C.c_int, [H, I32, I32, I32]),
+            "fw2v_batch_get_shape": (C.c_int, [H, I32, C.POINTER(I32), C.POINTER(I32)]),
+            "fw2v_batch_set_launch": (C.c_int, [H, I32, I32]),
+            "fw2v_batch_get_launch": (C.c_int, [H, C.POINTER(I32), C.POINTER(I32)]),
+            "fw2v_batch_tune": (C.c_int, [H, I64, C.POINTER(TuneReport)]),
+            "fw2v_batch_train": (C.c_int, [H, C.POINTER(BatchStats)]),
+            "fw2v_batch_job_words": (C.c_int, [H, I32, C.POINTER(U64), C.POINTER(U64)]),
+            "fw2v_batch_get_syn0": (C.c_int, [H, I32, P, I64]),
+            "fw2v_batch_get_syn1neg": (C.c_int, [H, I32, P, I64]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -298,3 +335,132 @@ class Trainer:
                                             _p(starts), _p(lens), len(lens), C.byref(loss),
                                             C.byref(pairs)), "heldout_loss")
         return loss.value, pairs.value
+
+
+class Batch:
+    """Many independent SGNS jobs trained together on one GPU (a libfw2v
+    batch): one persistent training kernel per round drains a work queue of
+    (job, sentence) items from every job.  Jobs need layer_size <= 128, the
+    table sigmoid and the same `negative`."""
+
+    def __init__(self, precision: int = FP32, device: int = 0, use_graph: bool = True,
+                 deterministic: bool = False, round_tokens: int = 0):
+        cfg = BatchConfig()
+        lib().fw2v_batch_config_default(C.byref(cfg))
+        cfg.precision, cfg.device = precision, device
+        cfg.use_graph, cfg.deterministic, cfg.round_tokens = int(use_graph), int(deterministic), round_tokens
+        h = C.c_void_p()
+        st = lib().fw2v_batch_create(C.byref(cfg), C.byref(h))
+        if st != 0:
+            raise Fw2vError(st, "fw2v_batch_create")
+        self._h = h
+        self.config = cfg
+        self.jobs: list[tuple[Config, int]] = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fw2v_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st: int, what: str):
+        if st != 0:
+            msg = lib().fw2v_batch_last_error(self._h)
+            raise Fw2vError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def add_job(self, config: Config, counts: np.ndarray, train_words: int, stream: np.ndarray,
+                chunk_off: np.ndarray) -> int:
+        counts = np.ascontiguousarray(counts, np.uint32)
+        stream = np.ascontiguousarray(stream, np.int32)
+        chunk_off = np.ascontiguousarray(chunk_off, np.int64)
+        j = C.c_int32()
+        self._check(lib().fw2v_batch_add_job(self._h, C.byref(config), _p(counts), len(counts), int(train_words),
+                                             _p(stream), len(stream), _p(chunk_off), len(chunk_off),
+                                             C.byref(j)), "batch_add_job")
+        self.jobs.append((config, len(counts)))
+        return j.value
+
+    def set_shape(self, job: int, lane_vec: int, stages: int):
+        self._check(lib().fw2v_batch_set_shape(self._h, job, lane_vec, stages), "batch_set_shape")
+
+    def shape(self, job: int) -> tuple[int, int]:
+        v, s = C.c_int32(), C.c_int32()
+        self._check(lib().fw2v_batch_get_shape(self._h, job, C.byref(v), C.byref(s)), "batch_get_shape")
+        return v.value, s.value
+
+    def set_launch(self, warps_per_block: int, blocks_per_sm: int = 0):
+        self._check(lib().fw2v_batch_set_launch(self._h, warps_per_block, blocks_per_sm), "batch_set_launch")
+
+    def launch(self) -> tuple[int, int]:
+        w, b = C.c_int32(), C.c_int32()
+        self._check(lib().fw2v_batch_get_launch(self._h, C.byref(w), C.byref(b)), "batch_get_launch")
+        return w.value, b.value
+
+    def tune(self, sample_tokens: int = 0, cache: str | None = None) -> dict:
+        """Pick every job class's shape and the grid by measurement
+        (fw2v_batch_tune).  With `cache`, a JSON file of earlier choices keyed
+        by device, precision and (d class, window, negative): classes found
+        there are applied without timing; if all are, nothing is timed."""
+        import json
+
+        keys = [self._class_key(c) for c, _ in self.jobs]
+        store = {}
+        if cache and os.path.exists(cache):
+            with open(cache) as f:
+                store = json.load(f)
+        if keys and all(k in store for k in keys) and "launch:" + self._device_key() in store:
+            for j, k in enumerate(keys):
+                self.set_shape(j, *store[k])
+            self.set_launch(*store["launch:" + self._device_key()])
+            return {"cached": True}
+        rep = TuneReport()
+        self._check(lib().fw2v_batch_tune(self._h, int(sample_tokens), C.byref(rep)), "batch_tune")
+        out = {"cached": False, "warps_per_block": rep.warps_per_block, "classes": []}
+        for c in range(rep.n_classes):
+            out["classes"].append({"d": rep.class_d[c], "window": rep.class_window[c],
+                                   "lane_vec": rep.class_lane_vec[c], "stages": rep.class_stages[c],
+                                   "tuned_wps": rep.tuned_wps[c], "default_wps": rep.default_wps[c]})
+        if cache:
+            for j, k in enumerate(keys):
+                store[k] = list(self.shape(j))
+            store["launch:" + self._device_key()] = list(self.launch())
+            with open(cache, "w") as f:
+                json.dump(store, f, indent=1, sort_keys=True)
+        return out
+
+    def _device_key(self) -> str:
+        return f"dev{self.config.device}:p{self.config.precision}"
+
+    def _class_key(self, c: Config) -> str:
+        pitch = (c.layer_size + 7) // 8 * 8
+        return f"{self._device_key()}:d{'64' if pitch <= 64 else '128'}:w{c.window}:k{c.negative}"
+
+    def train(self) -> BatchStats:
+        st = BatchStats()
+        self._check(lib().fw2v_batch_train(self._h, C.byref(st)), "batch_train")
+        return st
+
+    def job_words(self, job: int) -> tuple[int, int]:
+        r, k = C.c_uint64(), C.c_uint64()
+        self._check(lib().fw2v_batch_job_words(self._h, job, C.byref(r), C.byref(k)), "batch_job_words")
+        return r.value, k.value
+
+    def syn0(self, job: int) -> np.ndarray:
+        cfg, V = self.jobs[job]
+        out = np.zeros((V, cfg.layer_size), np.float32)
+        self._check(lib().fw2v_batch_get_syn0(self._h, job, _p(out), cfg.layer_size), "batch_get_syn0")
+        return out
+
+    def syn1neg(self, job: int) -> np.ndarray:
+        cfg, V = self.jobs[job]
+        out = np.zeros((V, cfg.layer_size), np.float32)
+        self._check(lib().fw2v_batch_get_syn1neg(self._h, job, _p(out), cfg.layer_size), "batch_get_syn1neg")
+        return out

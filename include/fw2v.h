@@ -79,6 +79,10 @@ typedef struct fw2v_config {
   int32_t precision;         /* fw2v_precision */
   int32_t deterministic;     /* 1: sentences trained one at a time in stream order */
   int32_t device;            /* CUDA device ordinal */
+  uint64_t seed;             /* 0: the reference's seeds (syn0 from LCG state 1,
+                                stream s from state s); otherwise syn0's start
+                                state, every stream's LCG and the stochastic-
+                                rounding seeds are offset by fw2v_seed_offset(seed) */
 } fw2v_config;
 
 typedef struct fw2v_handle fw2v_handle;
@@ -230,6 +234,87 @@ const char* fw2v_status_string(fw2v_status s);
 const char* fw2v_last_error(fw2v_handle* h);
 /* Library build information, e.g. "fw2v sm_100a". */
 const char* fw2v_version(void);
+
+/* ---- Batched training of many independent jobs ------------------------------
+ * No counterpart in the reference, which trains one corpus per process.  A
+ * batch holds many independent SGNS jobs (each its own vocabulary, corpus,
+ * layer size, window, seed and tables) and trains all of them on one GPU with
+ * one persistent training kernel per round: every epoch is cut into rounds of
+ * whole sampling streams of all jobs, sampled on the device (the same method,
+ * and for each job the same ids, negatives, learning rates and stochastic
+ * rounding seeds as a single-job handle with the same configuration) and then
+ * drained from one work queue of (job, sentence) items.  Sampling of round
+ * r+1 overlaps training of round r; with use_graph the whole call is captured
+ * and replayed as one CUDA graph.
+ *
+ * Jobs: layer_size <= 128, sigmoid FW2V_SIGMOID_TABLE, the same `negative` in
+ * every job of a batch; the batch's precision and deterministic flags replace
+ * the jobs' own. */
+typedef struct fw2v_batch fw2v_batch;
+
+typedef struct fw2v_batch_config {
+  int32_t precision;      /* fw2v_precision of every job's tables */
+  int32_t device;
+  int32_t use_graph;      /* 1: each fw2v_batch_train call runs as one CUDA graph */
+  int32_t deterministic;  /* 1: one warp trains every round's sentences in order */
+  int64_t round_tokens;   /* readable tokens sampled per round (buffer size); 0: 2^27 */
+} fw2v_batch_config;
+
+typedef struct fw2v_batch_stats {
+  uint64_t words_read;    /* tokens read by all jobs' streams in the call */
+  uint64_t words_kept;
+  float ms;               /* device time of the call (sampling and training) */
+  int32_t epochs;         /* epochs run: the largest job epoch count */
+  int32_t rounds;         /* rounds per epoch */
+} fw2v_batch_stats;
+
+void fw2v_batch_config_default(fw2v_batch_config* cfg);
+fw2v_status fw2v_batch_create(const fw2v_batch_config* cfg, fw2v_batch** out);
+void fw2v_batch_destroy(fw2v_batch* b);
+const char* fw2v_batch_last_error(fw2v_batch* b);
+
+/* Add a job: its configuration, vocabulary (as fw2v_set_vocab) and corpus (as
+ * fw2v_load_corpus, host memory).  Allocates and initialises its tables.
+ * *job receives its index (0, 1, ...). */
+fw2v_status fw2v_batch_add_job(fw2v_batch* b, const fw2v_config* cfg, const uint32_t* counts, int64_t vocab_size,
+                               uint64_t train_words, const int32_t* stream, int64_t stream_len,
+                               const int64_t* chunk_off, int64_t n_chunks, int32_t* job);
+
+/* A job's kernel shape: the lane vector width (2: 32 lanes of 2 floats cover
+ * d <= 64; 4: lanes of 4 floats cover d <= 128, 16 lanes suffice for d <= 64)
+ * and the pipeline stages (2, 3, 4 or 6 targets in flight).  Defaults follow
+ * d and negative; fw2v_batch_tune picks them by measurement. */
+fw2v_status fw2v_batch_set_shape(fw2v_batch* b, int32_t job, int32_t lane_vec, int32_t stages);
+fw2v_status fw2v_batch_get_shape(fw2v_batch* b, int32_t job, int32_t* lane_vec, int32_t* stages);
+
+/* The training grid: warps per block (sentences trained side by side in one
+ * block, 1..8) and a cap on blocks per SM (0: as many as fit). */
+fw2v_status fw2v_batch_set_launch(fw2v_batch* b, int32_t warps_per_block, int32_t blocks_per_sm);
+fw2v_status fw2v_batch_get_launch(fw2v_batch* b, int32_t* warps_per_block, int32_t* blocks_per_sm);
+
+/* Autotuner: for every class of jobs with the same (lane-vector class of d,
+ * window), time every shape on a sample of up to sample_tokens of the class's
+ * first-epoch sentences and keep the fastest; then time the grid shapes on
+ * all classes together.  Tables and sampler state are restored afterwards, so
+ * training is unchanged apart from speed.  Report: per class, the fastest
+ * words/s (tuned_wps) and the default shape's (default_wps), n_classes. */
+typedef struct fw2v_batch_tune_report {
+  int32_t n_classes;
+  int32_t class_d[16], class_window[16], class_lane_vec[16], class_stages[16];
+  double tuned_wps[16], default_wps[16];
+  int32_t warps_per_block, blocks_per_sm;
+} fw2v_batch_tune_report;
+fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2v_batch_tune_report* report);
+
+/* Train every job for its configured epochs (from the current state). */
+fw2v_status fw2v_batch_train(fw2v_batch* b, fw2v_batch_stats* stats);
+
+/* Words read and kept by one job since it was added. */
+fw2v_status fw2v_batch_job_words(fw2v_batch* b, int32_t job, uint64_t* words_read, uint64_t* words_kept);
+
+/* A job's tables as FP32 rows of ld floats (ld >= its layer_size). */
+fw2v_status fw2v_batch_get_syn0(fw2v_batch* b, int32_t job, float* out, int64_t ld);
+fw2v_status fw2v_batch_get_syn1neg(fw2v_batch* b, int32_t job, float* out, int64_t ld);
 
 #ifdef __cplusplus
 }

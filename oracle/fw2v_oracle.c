@@ -30,9 +30,9 @@ void orc_exp_table(float* t) {
   }
 }
 
-/* improved_driver_functions.cpp:27-31 */
-void orc_init_syn0(float* syn0, int64_t V, int d, int64_t pitch) {
-  uint64_t r = 1;
+/* improved_driver_functions.cpp:27-31, from LCG state `start` (1 there) */
+void orc_init_syn0_from(float* syn0, int64_t V, int d, int64_t pitch, uint64_t start) {
+  uint64_t r = start;
   for (int64_t row = 0; row < V; row++) {
     for (int c = 0; c < d; c++) {
       r = orc_lcg_next(r);
@@ -41,6 +41,8 @@ void orc_init_syn0(float* syn0, int64_t V, int d, int64_t pitch) {
     for (int64_t c = d; c < pitch; c++) syn0[row * pitch + c] = 0.0f;
   }
 }
+
+void orc_init_syn0(float* syn0, int64_t V, int d, int64_t pitch) { orc_init_syn0_from(syn0, V, d, pitch, 1); }
 
 /* improved_driver_functions.cpp:71-77: base = (float)(sample * train_words),
  * ratio = base / count, keep threshold = sqrtf(ratio) + ratio, all in float. */

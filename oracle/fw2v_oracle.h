@@ -39,6 +39,7 @@ void orc_exp_table(float* exp_table);
  * V*d row-major matrix takes ((r_i & 0xFFFF)/65536 - 0.5)/d with r_i the
  * (i+1)-th LCG state from seed 1.  Rows are written with `pitch` floats. */
 void orc_init_syn0(float* syn0, int64_t V, int d, int64_t pitch);
+void orc_init_syn0_from(float* syn0, int64_t V, int d, int64_t pitch, uint64_t start);
 
 /* Subsampling keep threshold (improved_driver_functions.cpp:71-77). */
 void orc_subsample_table(const uint32_t* counts, int64_t V, float sample, uint64_t train_words,

@@ -64,6 +64,7 @@ def _declare(L):
     L.orc_lcg_next.argtypes = [C.c_uint64]
     L.orc_exp_table.argtypes = [P]
     L.orc_init_syn0.argtypes = [P, C.c_int64, C.c_int, C.c_int64]
+    L.orc_init_syn0_from.argtypes = [P, C.c_int64, C.c_int, C.c_int64, C.c_uint64]
     L.orc_subsample_table.argtypes = [P, C.c_int64, C.c_float, C.c_uint64, P]
     L.orc_unigram_runs.restype = C.c_int64
     L.orc_unigram_runs.argtypes = [P, C.c_int64, C.c_int64, P, P, P]
@@ -108,9 +109,15 @@ def exp_table() -> np.ndarray:
     return t
 
 
-def init_syn0(V: int, d: int, pitch: int) -> np.ndarray:
+def seed_offset(seed: int) -> int:
+    """Offset of every LCG start state and stochastic-rounding seed for a
+    configuration's seed (the library's seed_offset; 0 keeps the reference's)."""
+    return mix64(seed) if seed else 0
+
+
+def init_syn0(V: int, d: int, pitch: int, seed: int = 0) -> np.ndarray:
     out = np.zeros((V, pitch), np.float32)
-    lib().orc_init_syn0(_p(out), V, d, pitch)
+    lib().orc_init_syn0_from(_p(out), V, d, pitch, (1 + seed_offset(seed)) & (2**64 - 1))
     return out
 
 
@@ -156,7 +163,7 @@ class StreamEpoch:
 
 def sample_streams(corpus: Corpus, *, threads: int, msl: int, negative: int, epochs: int,
                    alpha0: float, sample: float, table_size: int = UNIGRAM_TABLE_SIZE,
-                   runs=None):
+                   runs=None, seed: int = 0):
     """Run the reference batch builder for every stream and epoch.
 
     Returns out[stream][epoch] -> StreamEpoch.
@@ -177,6 +184,7 @@ def sample_streams(corpus: Corpus, *, threads: int, msl: int, negative: int, epo
     for s in range(threads):
         st = StreamState()
         L.orc_stream_init(C.byref(cfg), s, C.byref(st))
+        st.lcg = (st.lcg + seed_offset(seed)) & (2**64 - 1)
         a, b = C.c_int64(), C.c_int64()
         L.orc_stream_range(C.byref(cfg), s, C.byref(a), C.byref(b))
         cap = int(chunk_off[b.value] if b.value < len(chunk_off) else len(stream)) - \

@@ -44,6 +44,24 @@ def test_create_without_device_fails_cleanly():
     assert e.value.status == 6
 
 
+def test_batch_without_device_fails_cleanly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(fw2v.Fw2vError) as e:
+        fw2v.Batch()
+    assert e.value.status == 6
+    cfg = fw2v.BatchConfig()
+    fw2v.lib().fw2v_batch_config_default(C.byref(cfg))
+    assert (cfg.precision, cfg.use_graph, cfg.deterministic, cfg.round_tokens) == (fw2v.FP32, 1, 0, 0)
+    bad = fw2v.BatchConfig(precision=7)
+    assert fw2v.lib().fw2v_batch_create(C.byref(bad), C.byref(C.c_void_p())) == 1
+
+
+def test_default_config_seed_is_the_references():
+    assert fw2v.default_config().seed == 0
+
+
 def test_invalid_config_rejected_before_device_use():
     c = fw2v.default_config(window=16)
     h = C.c_void_p()
