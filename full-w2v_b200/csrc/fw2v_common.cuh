@@ -36,10 +36,12 @@ __host__ __device__ __forceinline__ Affine lcg_jump(uint64_t n) {
   return res;
 }
 
-// Counter-based random bits for stochastic rounding: a write-back event of a
-// training launch (seed), a sentence (uid) and an event within it (a target
-// row's or a leaving context row's write-back) gives a key; each vector of a
-// row then draws 64 bits from (key, row, vector), 16 per element.
+// Counter-based random bits for stochastic rounding.  A training launch
+// (seed) and a sentence (uid) give a 64-bit sentence key, once per sentence;
+// an event within the sentence (a target row's or a leaving context row's
+// write-back) and each vector of the row then draw their bits with 32-bit
+// multiply-xorshift steps: 32 bits per vector of 2 elements, 64 per vector of
+// 4, 16 per element.
 __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
   z += 0x9E3779B97F4A7C15ULL;
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
@@ -49,11 +51,25 @@ __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
 // Offset of every LCG start state and stochastic-rounding seed for a
 // configuration's seed (0 for seed 0: the reference's seeds).
 __host__ __device__ __forceinline__ uint64_t seed_offset(uint64_t seed) { return seed ? mix64(seed) : 0; }
-__host__ __device__ __forceinline__ uint64_t sr_event_key(uint64_t seed, uint64_t uid, uint64_t event) {
-  return mix64(seed ^ mix64(uid * 0x9E3779B97F4A7C15ULL + event));
+__host__ __device__ __forceinline__ uint32_t fmix32(uint32_t h) {
+  h ^= h >> 16;
+  h *= 0x85EBCA6Bu;
+  h ^= h >> 13;
+  h *= 0xC2B2AE35u;
+  h ^= h >> 16;
+  return h;
+}
+__host__ __device__ __forceinline__ uint64_t sr_sentence_key(uint64_t seed, uint64_t uid) {
+  return mix64(seed ^ mix64(uid * 0x9E3779B97F4A7C15ULL));
+}
+// Key of event `event` of a sentence: the low word mixed with the event number.
+__host__ __device__ __forceinline__ uint64_t sr_event_key(uint64_t skey, uint64_t event) {
+  return (skey & 0xFFFFFFFF00000000ULL) | (uint32_t)((uint32_t)skey ^ fmix32((uint32_t)event * 0x9E3779B9u + 1u));
 }
 __host__ __device__ __forceinline__ uint64_t sr_vector_bits(uint64_t key, uint64_t row, uint64_t vec) {
-  return mix64(key ^ (row * 0xD6E8FEB86659FD93ULL) ^ (vec + 1));
+  const uint32_t lo = fmix32((uint32_t)key ^ ((uint32_t)row * 0x27D4EB2Fu) ^ ((uint32_t)vec * 0x165667B1u));
+  const uint32_t hi = fmix32(lo ^ (uint32_t)(key >> 32));
+  return ((uint64_t)hi << 32) | lo;
 }
 // x rounded to bfloat16 up or down with probability proportional to the
 // distance (r16 uniform in [0, 65536)); NaN and infinity round to nearest.

@@ -590,6 +590,7 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   T* const syn1neg = reinterpret_cast<T*>(p.syn1neg);
   const float alpha = sn.alpha;
   const bool one_group = K + 1 <= R;
+  const uint64_t skey = sr_sentence_key(p.sr_seed, (uint64_t)sn.uid);  // bfloat16 tables only
 
   // Every id is checked before any table access.
   bool bad = L < 0;
@@ -725,7 +726,7 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
               Row<VEC, NV> o0;
               lds_row(o0, o0_b + (uint32_t)k * row_bytes, lm);
               row_add_delta(syn1neg + (int64_t)tk * P, o[k], o0, lane, d,
-                            sr_event_key(p.sr_seed, (uint64_t)sn.uid, (uint64_t)w * (K + 1) + (k0 + k)),
+                            sr_event_key(skey, (uint64_t)w * (K + 1) + (k0 + k)),
                             (uint64_t)tk);
             }
           }
@@ -748,7 +749,7 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
               sts_row(sv, a, lm);
             }
             row_add_delta(syn1neg + (int64_t)tk * P, so, so0, lane, d,
-                          sr_event_key(p.sr_seed, (uint64_t)sn.uid, (uint64_t)w * (K + 1) + (k0 + k)),
+                          sr_event_key(skey, (uint64_t)w * (K + 1) + (k0 + k)),
                           (uint64_t)tk);
           }
         }
@@ -762,7 +763,7 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
       lds_row(cur, ring_b + (uint32_t)(q_out % D) * row_bytes, lm);
       lds_staged<T>(org, out_b, lm);
       row_add_delta(syn0 + (int64_t)id_out * P, cur, org, lane, d,
-                    sr_event_key(p.sr_seed, (uint64_t)sn.uid, (uint64_t)L * (K + 1) + q_out), (uint64_t)id_out);
+                    sr_event_key(skey, (uint64_t)L * (K + 1) + q_out), (uint64_t)id_out);
     }
     if (id_in >= 0) {
       const int s = q_in % D;
@@ -781,7 +782,7 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
     row_load_global(org, orig + s * P, lane, d);
     const int id_q = __ldg(ids + q);
     row_add_delta(syn0 + (int64_t)id_q * P, cur, org, lane, d,
-                  sr_event_key(p.sr_seed, (uint64_t)sn.uid, (uint64_t)L * (K + 1) + q), (uint64_t)id_q);
+                  sr_event_key(skey, (uint64_t)L * (K + 1) + q), (uint64_t)id_q);
   }
 }
 
@@ -793,9 +794,16 @@ struct MinBlocks {
 };
 
 template <typename T, int VEC, int NV, int R, int SIG>
+// Sentences are taken one per warp: all by warp 0 in order (deterministic),
+// by static assignment (work_counter null: the kernel seam, whose launches
+// may run concurrently), or from an atomic work counter.  One call site of
+// train_sentence keeps the code (and the instruction cache footprint) to one
+// copy of the body; its parameters are read from a shared-memory copy.
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, MinBlocks<NV>::value) sgns_train_kernel(TrainParams p) {
   extern __shared__ __align__(16) float smem[];
-  const float* table = p.exp_table;
+  __shared__ __align__(8) TrainParams sp;
+  copy_params(&sp, &p, threadIdx.x, blockDim.x);
+  __syncthreads();
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int D = 2 * p.window + 1;
@@ -803,30 +811,24 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MinBlocks<NV>::value) sgn
   const int64_t gwarp = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
   T* orig = reinterpret_cast<T*>(p.orig_scratch) + gwarp * D * p.pitch;
   const int64_t total = total_sentences(p);
-  if (p.deterministic) {
-    if (blockIdx.x != 0 || warp != 0) return;
-    for (int64_t w = 0; w < total; w++) {
-      const Sentence sn = fetch_sentence(p, w);
-      train_sentence<T, VEC, NV, R, SIG>(p, sn, ring, orig, table, lane);
-    }
-    return;
-  }
-  if (p.work_counter == nullptr) {
-    // Static assignment (the kernel seam, whose launches may run concurrently).
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t w = gwarp; w < total; w += warps) {
-      const Sentence sn = fetch_sentence(p, w);
-      train_sentence<T, VEC, NV, R, SIG>(p, sn, ring, orig, table, lane);
-    }
-    return;
-  }
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  if (p.deterministic && gwarp != 0) return;
+  int64_t next = gwarp;
   for (;;) {
-    unsigned long long w = 0;
-    if (lane == 0) w = atomicAdd(p.work_counter, 1ULL);
-    w = __shfl_sync(kFull, w, 0);
-    if ((int64_t)w >= total) break;
-    const Sentence sn = fetch_sentence(p, (int64_t)w);
-    train_sentence<T, VEC, NV, R, SIG>(p, sn, ring, orig, table, lane);
+    int64_t w;
+    if (p.deterministic) {
+      w = next++;
+    } else if (p.work_counter == nullptr) {
+      w = next;
+      next += nwarps;
+    } else {
+      unsigned long long c = 0;
+      if (lane == 0) c = atomicAdd(p.work_counter, 1ULL);
+      w = (int64_t)__shfl_sync(kFull, c, 0);
+    }
+    if (w >= total) break;
+    const Sentence sn = fetch_sentence(p, w);
+    train_sentence<T, VEC, NV, R, SIG>(sp, sn, ring, orig, p.exp_table, lane);
   }
 }
 

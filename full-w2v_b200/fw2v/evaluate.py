@@ -18,13 +18,27 @@ import numpy as np
 from . import Trainer, default_config
 
 
+def sentence_chunks(stream: np.ndarray, msl: int) -> np.ndarray:
+    """Chunk starts of a token stream: every sentence (ended by a 0, or by the
+    end of the stream) cut into pieces of at most msl tokens."""
+    n = len(stream)
+    ends = np.nonzero(stream == 0)[0] + 1
+    if len(ends) == 0 or ends[-1] < n:
+        ends = np.concatenate([ends, [n]])
+    begins = np.concatenate([[0], ends[:-1]])
+    out = [np.arange(b, e, msl, dtype=np.int64) for b, e in zip(begins, ends) if e > b]
+    return np.concatenate(out) if out else np.zeros(1, np.int64)
+
+
 def heldout_pairs(counts, train_words, held_stream, *, window, negative, msl=1000, threads=16):
-    """(lens, ids, negs) of held-out sentences with K negatives per word."""
-    n_chunks = max(1, (len(held_stream) + msl - 1) // msl)
+    """(lens, ids, negs) of held-out sentences with K negatives per word.  A 0
+    in held_stream ends a sentence (walk corpora); otherwise sentences are
+    pieces of msl tokens."""
+    held = np.asarray(held_stream, np.int32)
+    chunk_off = sentence_chunks(held, msl)
     cfg = default_config(layer_size=8, window=window, negative=negative, epochs=1,
-                         threads=min(threads, n_chunks), msl=msl, sample=0.0)
-    stream = np.concatenate([np.asarray(held_stream, np.int32), [0]]).astype(np.int32)
-    chunk_off = np.arange(0, len(stream) - 1, msl, dtype=np.int64)
+                         threads=min(threads, len(chunk_off)), msl=msl, sample=0.0)
+    stream = np.concatenate([held, [0]]).astype(np.int32)
     with Trainer(cfg) as t:
         t.set_vocab(counts, train_words)
         t.load_corpus(stream, chunk_off)

@@ -306,3 +306,118 @@ def make_topic_corpus_gpu(name: str, *, n_tokens: int | None = None, heldout_tok
                                     min_count=cfg["min_count"], msl=msl, seed=1234 + int(name[1:]),
                                     device=device, heldout_tokens=heldout_tokens)
     return corpus, held, cfg
+
+
+def sbm_corpus_gpu(nodes: int, blocks: int, degree: float, p_ratio: float, walks_per_node: int, walk_len: int, *,
+                   seed: int = 0, device="cuda", min_count: int = 1, heldout_walks: int = 0):
+    """sbm_walks() generated with torch on a device, written as the reference's
+    text front end would read the walks one per line with -cache-eos: every
+    walk is a sentence ending in </s> and a stored chunk of its own.  The
+    vocabulary is the visited nodes by count (ties by first occurrence).
+
+    Returns (SynthCorpus with each node's block as its label and purity 1,
+    held-out walks as int32 vocab ids with a 0 after each, or None).
+    """
+    import torch
+
+    dev = torch.device(device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    block = (torch.arange(nodes, device=dev, dtype=torch.int64) * blocks) // nodes
+    bsize = nodes / blocks
+    p_out = degree / (p_ratio * (bsize - 1) + (nodes - bsize))
+    rng = np.random.default_rng(seed)
+    n_in = int(rng.poisson(p_ratio * p_out * (bsize - 1) * nodes / 2))
+    n_out = int(rng.poisson(p_out * (nodes - bsize) * nodes / 2))
+    a = torch.randint(0, nodes, (n_in,), device=dev, generator=gen)
+    lo = (block[a] * nodes) // blocks
+    hi = ((block[a] + 1) * nodes) // blocks
+    b = lo + (torch.rand(n_in, device=dev, generator=gen, dtype=torch.float64) * (hi - lo)).long()
+    c = torch.randint(0, nodes, (n_out,), device=dev, generator=gen)
+    d = torch.randint(0, nodes, (n_out,), device=dev, generator=gen)
+    keep = block[c] != block[d]
+    src = torch.cat([a, b, c[keep], d[keep]])
+    dst = torch.cat([b, a, d[keep], c[keep]])
+    ok = src != dst
+    src, dst = src[ok], dst[ok]
+    order = torch.argsort(src, stable=True)
+    src, dst = src[order], dst[order]
+    deg = torch.bincount(src, minlength=nodes)
+    offs = torch.zeros(nodes + 1, device=dev, dtype=torch.int64)
+    offs[1:] = torch.cumsum(deg, 0)
+    del a, b, c, d, keep, ok, order, src
+
+    def walk(starts):
+        out = torch.empty((len(starts), walk_len), device=dev, dtype=torch.int64)
+        cur = starts.clone()
+        out[:, 0] = cur
+        for t in range(1, walk_len):
+            dc = deg[cur]
+            pick = (torch.rand(len(cur), device=dev, generator=gen, dtype=torch.float64) * dc).long()
+            cur = torch.where(dc > 0, dst[offs[cur] + pick.clamp(max=(dc - 1).clamp(min=0))], cur)
+            out[:, t] = cur
+        return out
+
+    starts = torch.arange(nodes, device=dev, dtype=torch.int64).repeat_interleave(walks_per_node)
+    walks = walk(starts)
+    flat = walks.reshape(-1)
+    n = flat.numel()
+    cnt = torch.bincount(flat, minlength=nodes)
+    first = torch.full((nodes,), n, device=dev, dtype=torch.int64)
+    first.scatter_reduce_(0, flat, torch.arange(n, device=dev, dtype=torch.int64), reduce="amin")
+    seen = torch.nonzero(cnt).flatten()
+    vorder = seen[torch.argsort(first[seen], stable=True)]
+    vorder = vorder[torch.argsort(-cnt[vorder], stable=True)]
+    vorder = vorder[cnt[vorder] >= min_count]
+    vocab_of = torch.full((nodes,), -1, device=dev, dtype=torch.int64)
+    vocab_of[vorder] = torch.arange(1, len(vorder) + 1, device=dev)
+    n_walks = walks.shape[0]
+    counts = torch.cat([torch.tensor([max(n_walks - 1, 0)], device=dev), cnt[vorder]]).cpu().numpy().astype(np.uint32)
+
+    def lines(w):
+        ids = vocab_of[w]
+        ids = torch.cat([ids, torch.zeros((w.shape[0], 1), device=dev, dtype=torch.int64)], 1)
+        ids = ids.reshape(-1)
+        return ids[ids >= 0].to(torch.int32)
+
+    if min_count > 1:
+        raise ValueError("walk corpora keep every visited node (min_count 1)")
+    stream_t = lines(walks)
+    stream = torch.cat([stream_t, torch.zeros(1, device=dev, dtype=torch.int32)]).cpu().numpy()
+    chunk_off = np.arange(n_walks, dtype=np.int64) * (walk_len + 1)
+    label = np.concatenate([[-1], block[vorder].cpu().numpy()]).astype(np.int32)
+    raw_of_vocab = np.concatenate([[-1], vorder.cpu().numpy()]).astype(np.int64)
+    purity = np.concatenate([[0.0], np.ones(len(vorder))])
+    corpus = SynthCorpus(counts, int(counts.sum()) + 1, stream, chunk_off, label, raw_of_vocab, purity)
+    held = None
+    if heldout_walks:
+        hs = torch.randint(0, nodes, (heldout_walks,), device=dev, generator=gen)
+        hw = walk(hs)
+        held = lines(hw).cpu().numpy()
+    del walks, flat, stream_t
+    if dev.type == "cuda":
+        torch.cuda.empty_cache()
+    return corpus, held
+
+
+# Graph-walk workloads: C4 (one 1M-node graph) and the jobs of C5 (256 graphs of
+# log-uniform size), as specified for the benchmark configurations.
+GRAPH_CONFIGS = {
+    "c4": dict(nodes=1_000_000, blocks=64, degree=20.0, p_ratio=20.0, walks_per_node=10, walk_len=80, d=128,
+               window=10, negative=5, sample=1e-3, epochs=1),
+}
+
+
+def c5_job_specs(n_jobs: int = 256, seed: int = 5, scale: float = 1.0):
+    """Per-job specifications of the batched configuration: log-uniform 1k-200k
+    nodes (times `scale`), 4-64 blocks, average degree 10-30, 10 walks of 40-80
+    per node, d in {64, 128}, window in {5, 10}, negative 5, its own seed."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for j in range(n_jobs):
+        nodes = int(round(np.exp(rng.uniform(np.log(1_000), np.log(200_000))) * scale))
+        out.append(dict(nodes=max(nodes, 64), blocks=int(rng.integers(4, 65)), degree=float(rng.uniform(10, 30)),
+                        p_ratio=20.0, walks_per_node=10, walk_len=int(rng.integers(40, 81)),
+                        d=int(rng.choice([64, 128])), window=int(rng.choice([5, 10])), negative=5, sample=1e-3,
+                        epochs=1, seed=int(rng.integers(1, 2**31))))
+    return out

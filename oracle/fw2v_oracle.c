@@ -374,11 +374,26 @@ static uint64_t mix64(uint64_t z) {
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
   return z ^ (z >> 31);
 }
-static uint64_t sr_event_key(uint64_t seed, uint64_t uid, uint64_t event) {
-  return mix64(seed ^ mix64(uid * 0x9E3779B97F4A7C15ULL + event));
+static uint32_t fmix32(uint32_t h) {
+  h ^= h >> 16;
+  h *= 0x85EBCA6Bu;
+  h ^= h >> 13;
+  h *= 0xC2B2AE35u;
+  h ^= h >> 16;
+  return h;
+}
+/* The library's stochastic-rounding bits: a key per sentence, then 32-bit
+ * mixing per event and per vector of a row. */
+static uint64_t sr_sentence_key(uint64_t seed, uint64_t uid) {
+  return mix64(seed ^ mix64(uid * 0x9E3779B97F4A7C15ULL));
+}
+static uint64_t sr_event_key(uint64_t skey, uint64_t event) {
+  return (skey & 0xFFFFFFFF00000000ULL) | (uint32_t)((uint32_t)skey ^ fmix32((uint32_t)event * 0x9E3779B9u + 1u));
 }
 static uint64_t sr_vector_bits(uint64_t key, uint64_t row, uint64_t vec) {
-  return mix64(key ^ (row * 0xD6E8FEB86659FD93ULL) ^ (vec + 1));
+  uint32_t lo = fmix32((uint32_t)key ^ ((uint32_t)row * 0x27D4EB2Fu) ^ ((uint32_t)vec * 0x165667B1u));
+  uint32_t hi = fmix32(lo ^ (uint32_t)(key >> 32));
+  return ((uint64_t)hi << 32) | lo;
 }
 static float bf16_f(uint16_t h) {
   uint32_t b = (uint32_t)h << 16;
@@ -436,6 +451,7 @@ int orc_train_bf16(const orc_train_cfg* cfg, uint16_t* syn0, uint16_t* syn1, int
   for (int64_t s = 0; s < n_sent && rc == 0; s++) {
     const int L = lens[s];
     if (L <= 0) continue;
+    const uint64_t skey = sr_sentence_key(seed, (uint64_t)s);
     const int32_t* sid = ids + starts[s];
     const int32_t* sneg = negs + starts[s] * K;
     for (int p = 0; p < L; p++)
@@ -463,13 +479,13 @@ int orc_train_bf16(const orc_train_cfg* cfg, uint16_t* syn0, uint16_t* syn1, int
             }
           }
           bf16_writeback(syn1 + (int64_t)t * P, o, o0, d, cfg->vec,
-                         sr_event_key(seed, (uint64_t)s, (uint64_t)w * (K + 1) + k), (uint64_t)t);
+                         sr_event_key(skey, (uint64_t)w * (K + 1) + k), (uint64_t)t);
         }
       }
       if (w - W >= 0) {
         int p = w - W;
         bf16_writeback(syn0 + (int64_t)sid[p] * P, cur + (int64_t)p * d, orig + (int64_t)p * d, d, cfg->vec,
-                       sr_event_key(seed, (uint64_t)s, (uint64_t)L * (K + 1) + p), (uint64_t)sid[p]);
+                       sr_event_key(skey, (uint64_t)L * (K + 1) + p), (uint64_t)sid[p]);
       }
       if (w + W + 1 < L) {
         int p = w + W + 1;
@@ -478,7 +494,7 @@ int orc_train_bf16(const orc_train_cfg* cfg, uint16_t* syn0, uint16_t* syn1, int
     }
     for (int p = L - W > 0 ? L - W : 0; p < L; p++) {
       bf16_writeback(syn0 + (int64_t)sid[p] * P, cur + (int64_t)p * d, orig + (int64_t)p * d, d, cfg->vec,
-                     sr_event_key(seed, (uint64_t)s, (uint64_t)L * (K + 1) + p), (uint64_t)sid[p]);
+                     sr_event_key(skey, (uint64_t)L * (K + 1) + p), (uint64_t)sid[p]);
     }
   }
   free(cur);
