@@ -39,10 +39,14 @@ cudaError_t launch_sampler_round(const SamplerParams* d_jobs, const BatchRound& 
                                  const uint64_t* words, int n_jobs, int64_t* job_uid, int64_t* uid_base,
                                  unsigned long long* job_words, unsigned long long* job_kept,
                                  int64_t* entry_prefix, cudaStream_t st);
-extern template cudaError_t batch_grid<float>(int64_t, int, int, int, int64_t, int, int*, int*, size_t*);
-extern template cudaError_t batch_grid<bf16_t>(int64_t, int, int, int, int64_t, int, int*, int*, size_t*);
-extern template cudaError_t batch_launch<float>(const BatchTrainArgs&, int, int, size_t, cudaStream_t);
-extern template cudaError_t batch_launch<bf16_t>(const BatchTrainArgs&, int, int, size_t, cudaStream_t);
+extern template cudaError_t batch_grid<float, 0>(int64_t, int, int, int, int64_t, int, int*, int*, size_t*);
+extern template cudaError_t batch_grid<float, 1>(int64_t, int, int, int, int64_t, int, int*, int*, size_t*);
+extern template cudaError_t batch_grid<bf16_t, 0>(int64_t, int, int, int, int64_t, int, int*, int*, size_t*);
+extern template cudaError_t batch_grid<bf16_t, 1>(int64_t, int, int, int, int64_t, int, int*, int*, size_t*);
+extern template cudaError_t batch_launch<float, 0>(const BatchTrainArgs&, int, int, size_t, cudaStream_t);
+extern template cudaError_t batch_launch<float, 1>(const BatchTrainArgs&, int, int, size_t, cudaStream_t);
+extern template cudaError_t batch_launch<bf16_t, 0>(const BatchTrainArgs&, int, int, size_t, cudaStream_t);
+extern template cudaError_t batch_launch<bf16_t, 1>(const BatchTrainArgs&, int, int, size_t, cudaStream_t);
 }  // namespace fw2v
 
 using namespace fw2v;
@@ -65,11 +69,13 @@ struct BatchJob {
   int64_t n_chunks = 0;
   std::vector<int64_t> sbase;  // threads + 1: readable-token prefix of its streams
   int64_t gfirst = 0;          // global number of its stream 0
-  int lane_vec = 4, stages = 6;
+  int lane_vec = 4, lane_nv = 1, stages = 6;
   uint64_t epochs_done = 0;
+  int family() const { return lane_nv >= 2 ? 1 : 0; }
 };
 
 struct RoundPlan {
+  int family = 0;          // kernel family of all its jobs
   int n = 0;
   int64_t kept = 0;        // readable tokens of its streams
   int64_t max_region = 0;  // largest stream
@@ -94,20 +100,30 @@ struct RoundBuf {
   cudaEvent_t ready = nullptr, freed = nullptr;
 };
 
-// Lane vector widths and stage counts a job may use.
-bool valid_shape(int d, int vec, int stages) {
+// Lane layouts (vector width, vectors per lane) and stage counts a job of
+// layer size d may use: the lanes must cover d, no vector may lie wholly past
+// it, and wide rows use 4-float vectors.
+bool valid_shape(int d, int vec, int nv, int stages) {
   if (vec != 2 && vec != 4) return false;
-  if (d > 32 * vec) return false;
+  if (nv < 1 || nv > 3 || (nv > 1 && vec != 4)) return false;
+  if (d > 32 * vec * nv || (nv > 1 && d <= 32 * vec * (nv - 1))) return false;
+  if (nv >= 3 && stages > 4) return false;  // no 6-stage body for rows of three vectors
   for (int s : kBatchStages)
     if (s == stages) return true;
   return false;
 }
 
-// Default stages: the fewest groups of targets per centre, then the fewest idle stages.
-int default_stages(int negative) {
+// Layout class of a layer size: d <= 64, <= 128, <= 256, <= 384.
+int layout_class(int64_t pitch) { return pitch <= 64 ? 0 : pitch <= 128 ? 1 : pitch <= 256 ? 2 : 3; }
+
+// Default stages: the fewest groups of targets per centre, then the fewest
+// idle stages; rows of three vectors per lane stop at 4 (their 6-stage body
+// does not fit the register file).
+int default_stages(int negative, int nv = 1) {
   const int t = negative + 1;
   int best = 6, best_groups = 1 << 30, best_idle = 1 << 30;
   for (int s : kBatchStages) {
+    if (nv >= 3 && s > 4) continue;
     const int g = (t + s - 1) / s, idle = g * s - t;
     if (g < best_groups || (g == best_groups && idle < best_idle)) {
       best = s;
@@ -152,7 +168,7 @@ struct fw2v_batch {
   int64_t buf_kept_cap = 0, buf_stream_cap = 0;
   void* orig_scratch = nullptr;
   int64_t scratch_elems = 0, scratch_warps = 0, scratch_bytes = 0;
-  int warps_per_block = 4, blocks_per_sm = 0;
+  int warps_per_block[2] = {4, 4}, blocks_per_sm[2] = {0, 0};  // per kernel family
 };
 
 namespace {
@@ -284,6 +300,7 @@ TrainParams train_params(const fw2v_batch* b, const BatchJob& j, const RoundBuf&
   p.sr_seed = j.soff + j.epochs_done;
   p.bf16 = b->elem == 2;
   p.lane_vec = j.lane_vec;
+  p.lane_nv = j.lane_nv;
   p.stages = j.stages;
   return p;
 }
@@ -297,21 +314,25 @@ fw2v_status plan(fw2v_batch* b) {
     int32_t job, local;
     int64_t gstream, tokens;
   };
+  const int64_t cap = b->cfg.round_tokens > 0 ? b->cfg.round_tokens : (int64_t)1 << 27;
+  for (int fam = 0; fam < 2; fam++) {
   std::vector<Item> order;
   int max_t = 0;
-  for (const BatchJob& j : b->jobs) max_t = std::max(max_t, j.cfg.threads);
+  for (const BatchJob& j : b->jobs)
+    if (j.family() == fam) max_t = std::max(max_t, j.cfg.threads);
   for (int s = 0; s < max_t; s++)
     for (size_t ji = 0; ji < b->jobs.size(); ji++) {
       const BatchJob& j = b->jobs[ji];
-      if (s < j.cfg.threads) order.push_back({(int32_t)ji, s, j.gfirst + s, j.sbase[s + 1] - j.sbase[s]});
+      if (j.family() == fam && s < j.cfg.threads)
+        order.push_back({(int32_t)ji, s, j.gfirst + s, j.sbase[s + 1] - j.sbase[s]});
     }
-  const int64_t cap = b->cfg.round_tokens > 0 ? b->cfg.round_tokens : (int64_t)1 << 27;
   size_t i = 0;
   while (i < order.size()) {
     size_t e = i;
     int64_t tok = 0;
     while (e < order.size() && (e == i || (tok + order[e].tokens <= cap && e - i < 65535))) tok += order[e++].tokens;
     RoundPlan r;
+    r.family = fam;
     r.n = (int)(e - i);
     std::vector<int32_t> job(r.n), local(r.n);
     std::vector<int64_t> gs(r.n), kb(r.n + 1, 0);
@@ -340,6 +361,7 @@ fw2v_status plan(fw2v_batch* b) {
     b->buf_kept_cap = std::max(b->buf_kept_cap, r.kept);
     b->buf_stream_cap = std::max<int64_t>(b->buf_stream_cap, r.n);
     i = e;
+  }
   }
   const int64_t kc = std::max<int64_t>(b->buf_kept_cap, 1), sc = b->buf_stream_cap;
   const int K = std::max(b->negative, 1);
@@ -395,14 +417,24 @@ struct Grid {
   int64_t smem_floats = 0;
 };
 
-fw2v_status grid_for(fw2v_batch* b, const std::vector<int>& active, int wpb, int cap, Grid* g) {
+// Grid of kernel family `fam` for the jobs `active` of that family.
+fw2v_status grid_for(fw2v_batch* b, const std::vector<int>& active, int fam, int wpb, int cap, Grid* g) {
   g->smem_floats = 0;
-  for (int j : active) g->smem_floats = std::max(g->smem_floats, shape_smem_floats(b->jobs[j]));
-  const cudaError_t e =
-      b->elem == 2 ? batch_grid<bf16_t>(g->smem_floats, wpb, cap, b->num_sms, b->scratch_warps, b->cfg.deterministic,
-                                        &g->blocks, &g->threads, &g->smem)
-                   : batch_grid<float>(g->smem_floats, wpb, cap, b->num_sms, b->scratch_warps, b->cfg.deterministic,
-                                       &g->blocks, &g->threads, &g->smem);
+  for (int j : active)
+    if (b->jobs[j].family() == fam) g->smem_floats = std::max(g->smem_floats, shape_smem_floats(b->jobs[j]));
+  if (g->smem_floats == 0) return FW2V_OK;
+  const int det = b->cfg.deterministic;
+  cudaError_t e;
+  if (b->elem == 2)
+    e = fam ? batch_grid<bf16_t, 1>(g->smem_floats, wpb, cap, b->num_sms, b->scratch_warps, det, &g->blocks,
+                                    &g->threads, &g->smem)
+            : batch_grid<bf16_t, 0>(g->smem_floats, wpb, cap, b->num_sms, b->scratch_warps, det, &g->blocks,
+                                    &g->threads, &g->smem);
+  else
+    e = fam ? batch_grid<float, 1>(g->smem_floats, wpb, cap, b->num_sms, b->scratch_warps, det, &g->blocks,
+                                   &g->threads, &g->smem)
+            : batch_grid<float, 0>(g->smem_floats, wpb, cap, b->num_sms, b->scratch_warps, det, &g->blocks,
+                                   &g->threads, &g->smem);
   if (e != cudaSuccess)
     return bfail(b, FW2V_ERR_ARGUMENT, "batch grid (%d warps per block, %lld floats per warp): %s", wpb,
                  (long long)g->smem_floats, cudaGetErrorString(e));
@@ -429,9 +461,13 @@ BatchTrainArgs train_args(const fw2v_batch* b, const RoundBuf& rb, const BatchRo
   return a;
 }
 
-cudaError_t launch_train_round(const fw2v_batch* b, const BatchTrainArgs& a, const Grid& g, cudaStream_t st) {
-  return b->elem == 2 ? batch_launch<bf16_t>(a, g.blocks, g.threads, g.smem, st)
-                      : batch_launch<float>(a, g.blocks, g.threads, g.smem, st);
+cudaError_t launch_train_round(const fw2v_batch* b, int fam, const BatchTrainArgs& a, const Grid& g,
+                               cudaStream_t st) {
+  if (b->elem == 2)
+    return fam ? batch_launch<bf16_t, 1>(a, g.blocks, g.threads, g.smem, st)
+               : batch_launch<bf16_t, 0>(a, g.blocks, g.threads, g.smem, st);
+  return fam ? batch_launch<float, 1>(a, g.blocks, g.threads, g.smem, st)
+             : batch_launch<float, 0>(a, g.blocks, g.threads, g.smem, st);
 }
 
 // Sample one round into buffer set rb on the sampler stream.
@@ -443,7 +479,7 @@ cudaError_t enqueue_sample(fw2v_batch* b, RoundBuf& rb, const BatchRound& r, int
 
 // Every round of `epochs` epochs: sampler stream and training stream joined
 // by events, ending with the sampler stream joined into the training stream.
-cudaError_t enqueue_epochs(fw2v_batch* b, int epochs, const Grid& g) {
+cudaError_t enqueue_epochs(fw2v_batch* b, int epochs, const Grid* grids) {
   cudaError_t e = cudaEventRecord(b->ev_fork, b->st);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(b->sst, b->ev_fork, 0);
   int64_t k = 0;
@@ -457,7 +493,8 @@ cudaError_t enqueue_epochs(fw2v_batch* b, int epochs, const Grid& g) {
       if (e == cudaSuccess) e = cudaEventRecord(rb.ready, b->sst);
       if (e == cudaSuccess) e = cudaStreamWaitEvent(b->st, rb.ready, 0);
       if (e == cudaSuccess) e = cudaMemsetAsync(b->counter, 0, sizeof(unsigned long long), b->st);
-      if (e == cudaSuccess) e = launch_train_round(b, train_args(b, rb, r.view, ep, g), g, b->st);
+      const Grid& g = grids[r.family];
+      if (e == cudaSuccess) e = launch_train_round(b, r.family, train_args(b, rb, r.view, ep, g), g, b->st);
       if (e == cudaSuccess) e = cudaEventRecord(rb.freed, b->st);
     }
   }
@@ -573,11 +610,11 @@ fw2v_status fw2v_batch_add_job(fw2v_batch* b, const fw2v_config* cfg, const uint
                                const int64_t* chunk_off, int64_t n_chunks, int32_t* job_out) {
   if (!b || !cfg || !counts || !stream || !chunk_off) return bfail(b, FW2V_ERR_ARGUMENT, "null argument");
   const fw2v_config& c = *cfg;
-  if (c.layer_size < 1 || c.layer_size > 128 || c.window < 1 || c.window > kMaxWindow || c.negative < 0 ||
+  if (c.layer_size < 1 || c.layer_size > 384 || c.window < 1 || c.window > kMaxWindow || c.negative < 0 ||
       c.negative > kMaxNegative || c.epochs < 0 || c.threads < 1 || c.msl < 1 || !(c.alpha > 0) ||
       !(c.sample >= 0) || c.sigmoid != FW2V_SIGMOID_TABLE)
     return bfail(b, FW2V_ERR_ARGUMENT,
-                 "batch job: layer_size 1..128, window 1..15, negative 0..31, table sigmoid required");
+                 "batch job: layer_size 1..384, window 1..15, negative 0..31, table sigmoid required");
   if (b->negative >= 0 && c.negative != b->negative)
     return bfail(b, FW2V_ERR_ARGUMENT, "batch job: negative %d differs from the batch's %d", c.negative, b->negative);
   if (V < 2 || V > (int64_t)INT32_MAX) return bfail(b, FW2V_ERR_ARGUMENT, "batch job: V >= 2 required");
@@ -598,7 +635,8 @@ fw2v_status fw2v_batch_add_job(fw2v_batch* b, const fw2v_config* cfg, const uint
   j.pitch = ((int64_t)c.layer_size + 7) / 8 * 8;
   j.soff = seed_offset(c.seed);
   j.lane_vec = j.pitch <= 64 ? 2 : 4;
-  j.stages = default_stages(c.negative);
+  j.lane_nv = j.pitch <= 128 ? 1 : (j.pitch <= 256 ? 2 : 3);
+  j.stages = default_stages(c.negative, j.lane_nv);
   j.stream_len = stream_len;
   j.n_chunks = n_chunks;
   auto undo = [&](fw2v_status s) {
@@ -696,36 +734,40 @@ fw2v_status fw2v_batch_add_job(fw2v_batch* b, const fw2v_config* cfg, const uint
   return FW2V_OK;
 }
 
-fw2v_status fw2v_batch_set_shape(fw2v_batch* b, int32_t job, int32_t lane_vec, int32_t stages) {
+fw2v_status fw2v_batch_set_shape(fw2v_batch* b, int32_t job, int32_t lane_vec, int32_t lane_nv, int32_t stages) {
   if (!b || job < 0 || job >= (int32_t)b->jobs.size()) return bfail(b, FW2V_ERR_ARGUMENT, "bad job");
   BatchJob& j = b->jobs[job];
-  if (!valid_shape(j.cfg.layer_size, lane_vec, stages))
-    return bfail(b, FW2V_ERR_ARGUMENT, "shape (%d, %d) cannot train d = %d", lane_vec, stages, j.cfg.layer_size);
+  if (!valid_shape(j.cfg.layer_size, lane_vec, lane_nv, stages))
+    return bfail(b, FW2V_ERR_ARGUMENT, "shape (%d x %d, %d stages) cannot train d = %d", lane_vec, lane_nv, stages,
+                 j.cfg.layer_size);
+  if ((lane_nv >= 2) != (j.family() == 1)) b->planned = false;  // the job moves to the other kernel family
   j.lane_vec = lane_vec;
+  j.lane_nv = lane_nv;
   j.stages = stages;
   return FW2V_OK;
 }
 
-fw2v_status fw2v_batch_get_shape(fw2v_batch* b, int32_t job, int32_t* lane_vec, int32_t* stages) {
-  if (!b || job < 0 || job >= (int32_t)b->jobs.size() || !lane_vec || !stages)
+fw2v_status fw2v_batch_get_shape(fw2v_batch* b, int32_t job, int32_t* lane_vec, int32_t* lane_nv, int32_t* stages) {
+  if (!b || job < 0 || job >= (int32_t)b->jobs.size() || !lane_vec || !lane_nv || !stages)
     return bfail(b, FW2V_ERR_ARGUMENT, "bad job");
   *lane_vec = b->jobs[job].lane_vec;
+  *lane_nv = b->jobs[job].lane_nv;
   *stages = b->jobs[job].stages;
   return FW2V_OK;
 }
 
-fw2v_status fw2v_batch_set_launch(fw2v_batch* b, int32_t warps_per_block, int32_t blocks_per_sm) {
-  if (!b || warps_per_block < 1 || warps_per_block > kBatchMaxWarps || blocks_per_sm < 0)
-    return bfail(b, FW2V_ERR_ARGUMENT, "warps per block 1..8, blocks per SM >= 0");
-  b->warps_per_block = warps_per_block;
-  b->blocks_per_sm = blocks_per_sm;
+fw2v_status fw2v_batch_set_launch(fw2v_batch* b, int32_t family, int32_t warps_per_block, int32_t blocks_per_sm) {
+  if (!b || family < 0 || family > 1 || warps_per_block < 1 || warps_per_block > kBatchMaxWarps || blocks_per_sm < 0)
+    return bfail(b, FW2V_ERR_ARGUMENT, "family 0 or 1, warps per block 1..8, blocks per SM >= 0");
+  b->warps_per_block[family] = warps_per_block;
+  b->blocks_per_sm[family] = blocks_per_sm;
   return FW2V_OK;
 }
 
-fw2v_status fw2v_batch_get_launch(fw2v_batch* b, int32_t* warps_per_block, int32_t* blocks_per_sm) {
-  if (!b || !warps_per_block || !blocks_per_sm) return FW2V_ERR_ARGUMENT;
-  *warps_per_block = b->warps_per_block;
-  *blocks_per_sm = b->blocks_per_sm;
+fw2v_status fw2v_batch_get_launch(fw2v_batch* b, int32_t family, int32_t* warps_per_block, int32_t* blocks_per_sm) {
+  if (!b || family < 0 || family > 1 || !warps_per_block || !blocks_per_sm) return FW2V_ERR_ARGUMENT;
+  *warps_per_block = b->warps_per_block[family];
+  *blocks_per_sm = b->blocks_per_sm[family];
   return FW2V_OK;
 }
 
@@ -738,9 +780,11 @@ fw2v_status fw2v_batch_train(fw2v_batch* b, fw2v_batch_stats* stats) {
   if (s != FW2V_OK) return s;
   std::vector<int> all(b->jobs.size());
   for (size_t i = 0; i < all.size(); i++) all[i] = (int)i;
-  Grid g;
-  s = grid_for(b, all, b->warps_per_block, b->blocks_per_sm, &g);
-  if (s != FW2V_OK) return s;
+  Grid g[2];
+  for (int fam = 0; fam < 2; fam++) {
+    s = grid_for(b, all, fam, b->warps_per_block[fam], b->blocks_per_sm[fam], &g[fam]);
+    if (s != FW2V_OK) return s;
+  }
   int epochs = 0;
   for (const BatchJob& j : b->jobs) epochs = std::max(epochs, j.cfg.epochs);
   const size_t J = b->jobs.size();
@@ -832,24 +876,25 @@ fw2v_status tuning_round(fw2v_batch* b, const std::vector<int>& jobs, int64_t to
   return FW2V_OK;
 }
 
-// Train the round sampled in buf[0] `reps` times; the fastest time in ms.
-fw2v_status time_round(fw2v_batch* b, const RoundPlan& r, const std::vector<int>& active, int wpb, int cap,
+// Train the round sampled in buf[0] (jobs of kernel family `fam`) `reps`
+// times after one warm-up; the fastest time in ms.
+fw2v_status time_round(fw2v_batch* b, const RoundPlan& r, const std::vector<int>& active, int fam, int wpb, int cap,
                        int reps, float* best_ms) {
   fw2v_status s = upload_params(b);
   if (s != FW2V_OK) return s;
   Grid g;
-  s = grid_for(b, active, wpb, cap, &g);
+  s = grid_for(b, active, fam, wpb, cap, &g);
   if (s != FW2V_OK) return s;
   *best_ms = 1e30f;
   for (int i = 0; i <= reps; i++) {
     BCK(b, cudaMemsetAsync(b->counter, 0, sizeof(unsigned long long), b->st));
     BCK(b, cudaEventRecord(b->ev_start, b->st));
-    BCK(b, launch_train_round(b, train_args(b, b->buf[0], r.view, 0, g), g, b->st));
+    BCK(b, launch_train_round(b, fam, train_args(b, b->buf[0], r.view, 0, g), g, b->st));
     BCK(b, cudaEventRecord(b->ev_end, b->st));
     BCK(b, cudaStreamSynchronize(b->st));
     float ms = 0;
     BCK(b, cudaEventElapsedTime(&ms, b->ev_start, b->ev_end));
-    if (i > 0) *best_ms = std::min(*best_ms, ms);  // the first run warms up
+    if (i > 0) *best_ms = std::min(*best_ms, ms);
   }
   return FW2V_OK;
 }
@@ -864,11 +909,12 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
   if (s != FW2V_OK) return s;
   if (sample_tokens <= 0) sample_tokens = (int64_t)1 << 23;
   const size_t J = b->jobs.size();
-  // classes of jobs with the same (lane-vector class of d, window)
+  // classes of jobs with the same (layout class of d, window); a class's
+  // layouts all belong to one kernel family
   std::vector<std::pair<int, int>> keys;
   std::vector<std::vector<int>> members;
   for (size_t i = 0; i < J; i++) {
-    const std::pair<int, int> k{b->jobs[i].pitch <= 64 ? 0 : 1, b->jobs[i].cfg.window};
+    const std::pair<int, int> k{layout_class(b->jobs[i].pitch), b->jobs[i].cfg.window};
     size_t c = std::find(keys.begin(), keys.end(), k) - keys.begin();
     if (c == keys.size()) {
       keys.push_back(k);
@@ -886,19 +932,49 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
   float* s_alpha = nullptr;
   BCK(b, cudaStreamSynchronize(b->st));
   BCK(b, cudaMalloc(&snap, tbytes));
-  size_t off = 0;
-  for (const BatchJob& j : b->jobs) {
-    const size_t tb = (size_t)j.V * j.pitch * b->elem;
-    BCK(b, cudaMemcpy(snap + off, j.syn0, tb, cudaMemcpyDeviceToDevice));
-    BCK(b, cudaMemcpy(snap + off + tb, j.syn1neg, tb, cudaMemcpyDeviceToDevice));
-    off += 2 * tb;
+  auto restore = [&]() {
+    size_t off = 0;
+    for (const BatchJob& j : b->jobs) {
+      const size_t tb = (size_t)j.V * j.pitch * b->elem;
+      cudaMemcpy(j.syn0, snap + off, tb, cudaMemcpyDeviceToDevice);
+      cudaMemcpy(j.syn1neg, snap + off + tb, tb, cudaMemcpyDeviceToDevice);
+      off += 2 * tb;
+    }
+    if (s_lcg && s_wca && s_alpha) {
+      cudaMemcpy(b->lcg, s_lcg, b->n_gstreams * 8, cudaMemcpyDeviceToDevice);
+      cudaMemcpy(b->wca, s_wca, b->n_gstreams * 8, cudaMemcpyDeviceToDevice);
+      cudaMemcpy(b->alpha, s_alpha, b->n_gstreams * 4, cudaMemcpyDeviceToDevice);
+    }
+    const cudaError_t e = cudaDeviceSynchronize();
+    bfree(snap);
+    bfree(s_lcg);
+    bfree(s_wca);
+    bfree(s_alpha);
+    return e;
+  };
+  {
+    size_t off = 0;
+    cudaError_t e = cudaSuccess;
+    for (const BatchJob& j : b->jobs) {
+      const size_t tb = (size_t)j.V * j.pitch * b->elem;
+      if (e == cudaSuccess) e = cudaMemcpy(snap + off, j.syn0, tb, cudaMemcpyDeviceToDevice);
+      if (e == cudaSuccess) e = cudaMemcpy(snap + off + tb, j.syn1neg, tb, cudaMemcpyDeviceToDevice);
+      off += 2 * tb;
+    }
+    if (e == cudaSuccess) e = balloc(s_lcg, b->n_gstreams);
+    if (e == cudaSuccess) e = balloc(s_wca, b->n_gstreams);
+    if (e == cudaSuccess) e = balloc(s_alpha, b->n_gstreams);
+    if (e == cudaSuccess) e = cudaMemcpy(s_lcg, b->lcg, b->n_gstreams * 8, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s_wca, b->wca, b->n_gstreams * 8, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s_alpha, b->alpha, b->n_gstreams * 4, cudaMemcpyDeviceToDevice);
+    if (e != cudaSuccess) {
+      bfree(snap);
+      bfree(s_lcg);
+      bfree(s_wca);
+      bfree(s_alpha);
+      return bfail(b, FW2V_ERR_NOMEM, "tuning snapshot: %s", cudaGetErrorString(e));
+    }
   }
-  BCK(b, balloc(s_lcg, b->n_gstreams));
-  BCK(b, balloc(s_wca, b->n_gstreams));
-  BCK(b, balloc(s_alpha, b->n_gstreams));
-  BCK(b, cudaMemcpy(s_lcg, b->lcg, b->n_gstreams * 8, cudaMemcpyDeviceToDevice));
-  BCK(b, cudaMemcpy(s_wca, b->wca, b->n_gstreams * 8, cudaMemcpyDeviceToDevice));
-  BCK(b, cudaMemcpy(s_alpha, b->alpha, b->n_gstreams * 4, cudaMemcpyDeviceToDevice));
 
   fw2v_batch_tune_report rep{};
   rep.n_classes = (int32_t)keys.size();
@@ -908,8 +984,6 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
     BCK(b, cudaMemsetAsync(b->job_uid, 0, J * sizeof(int64_t), b->sst));
     BCK(b, enqueue_sample(b, b->buf[0], r.view, r.max_region, 0));
     BCK(b, cudaStreamSynchronize(b->sst));
-    int64_t total = 0;
-    BCK(b, cudaMemcpy(&total, b->buf[0].entry_prefix + r.n, 8, cudaMemcpyDeviceToHost));
     return check_error_flag(b, "batch tune sampling");
   };
   auto kept_of = [&](const RoundPlan& r, double* kept) -> fw2v_status {
@@ -928,19 +1002,22 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
     if (result == FW2V_OK) result = kept_of(r, &kept);
     int d_max = 0;
     for (int j : members[c]) d_max = std::max(d_max, b->jobs[j].cfg.layer_size);
-    const int def_vec = b->jobs[members[c][0]].pitch <= 64 ? 2 : 4;
-    const int def_st = default_stages(b->negative);
+    const BatchJob& j0 = b->jobs[members[c][0]];
+    const int def_vec = j0.pitch <= 64 ? 2 : 4, def_nv = j0.pitch <= 128 ? 1 : (j0.pitch <= 256 ? 2 : 3);
+    const int def_st = default_stages(b->negative, def_nv);
+    const int fam = def_nv >= 2 ? 1 : 0;
     double best = -1, def_wps = 0;
-    int best_vec = def_vec, best_st = def_st;
+    int best_vec = def_vec, best_nv = def_nv, best_st = def_st;
     for (int vec : {2, 4}) {
-      if (result != FW2V_OK || !valid_shape(d_max, vec, 2)) continue;
       for (int st : kBatchStages) {
+        if (result != FW2V_OK || !valid_shape(d_max, vec, def_nv, st)) continue;
         for (int j : members[c]) {
           b->jobs[j].lane_vec = vec;
+          b->jobs[j].lane_nv = def_nv;
           b->jobs[j].stages = st;
         }
         float ms = 0;
-        result = time_round(b, r, members[c], b->warps_per_block, b->blocks_per_sm, 2, &ms);
+        result = time_round(b, r, members[c], fam, b->warps_per_block[fam], b->blocks_per_sm[fam], 2, &ms);
         if (result != FW2V_OK) break;
         const double wps = kept / (ms / 1e3);
         if (vec == def_vec && st == def_st) def_wps = wps;
@@ -953,60 +1030,52 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
     }
     for (int j : members[c]) {
       b->jobs[j].lane_vec = best_vec;
+      b->jobs[j].lane_nv = best_nv;
       b->jobs[j].stages = best_st;
     }
     rep.class_d[c] = d_max;
     rep.class_window[c] = keys[c].second;
     rep.class_lane_vec[c] = best_vec;
+    rep.class_lane_nv[c] = best_nv;
     rep.class_stages[c] = best_st;
     rep.tuned_wps[c] = best;
     rep.default_wps[c] = def_wps;
     bfree(r.dev);
   }
-  // grid: warps per block over all jobs together
-  if (result == FW2V_OK) {
-    std::vector<int> all(J);
-    for (size_t i = 0; i < J; i++) all[i] = (int)i;
+  // grid of each kernel family: warps per block over all its jobs together
+  for (int fam = 0; fam < 2 && result == FW2V_OK; fam++) {
+    std::vector<int> act;
+    for (size_t i = 0; i < J; i++)
+      if (b->jobs[i].family() == fam) act.push_back((int)i);
+    if (act.empty()) continue;
+    int n_cls = 0;
+    for (size_t c = 0; c < keys.size(); c++) n_cls += (keys[c].first >= 2) == (fam == 1);
     RoundPlan r;
-    result = tuning_round(b, all, sample_tokens * (int64_t)keys.size(), &r);
+    result = tuning_round(b, act, sample_tokens * (int64_t)std::max(n_cls, 1), &r);
     if (result == FW2V_OK) result = sample_into_buf0(r);
     double best = -1;
-    int best_w = b->warps_per_block;
+    int best_w = b->warps_per_block[fam];
     for (int w : {2, 4, 8}) {
       if (result != FW2V_OK) break;
-      float ms = 0;
       Grid g;
-      if (grid_for(b, all, w, 0, &g) != FW2V_OK) continue;  // does not fit: skip
-      result = time_round(b, r, all, w, 0, 2, &ms);
+      if (grid_for(b, act, fam, w, 0, &g) != FW2V_OK) continue;  // does not fit: skip
+      float ms = 0;
+      result = time_round(b, r, act, fam, w, 0, 2, &ms);
       if (result == FW2V_OK && 1.0 / ms > best) {
         best = 1.0 / ms;
         best_w = w;
       }
     }
-    b->warps_per_block = best_w;
-    b->blocks_per_sm = 0;
+    b->warps_per_block[fam] = best_w;
+    b->blocks_per_sm[fam] = 0;
     bfree(r.dev);
   }
-  rep.warps_per_block = b->warps_per_block;
-  rep.blocks_per_sm = b->blocks_per_sm;
-  // restore
-  cudaStreamSynchronize(b->st);
-  cudaStreamSynchronize(b->sst);
-  off = 0;
-  for (const BatchJob& j : b->jobs) {
-    const size_t tb = (size_t)j.V * j.pitch * b->elem;
-    cudaMemcpy(j.syn0, snap + off, tb, cudaMemcpyDeviceToDevice);
-    cudaMemcpy(j.syn1neg, snap + off + tb, tb, cudaMemcpyDeviceToDevice);
-    off += 2 * tb;
+  for (int fam = 0; fam < 2; fam++) {
+    rep.warps_per_block[fam] = b->warps_per_block[fam];
+    rep.blocks_per_sm[fam] = b->blocks_per_sm[fam];
   }
-  cudaMemcpy(b->lcg, s_lcg, b->n_gstreams * 8, cudaMemcpyDeviceToDevice);
-  cudaMemcpy(b->wca, s_wca, b->n_gstreams * 8, cudaMemcpyDeviceToDevice);
-  cudaMemcpy(b->alpha, s_alpha, b->n_gstreams * 4, cudaMemcpyDeviceToDevice);
-  const cudaError_t e = cudaDeviceSynchronize();
-  bfree(snap);
-  bfree(s_lcg);
-  bfree(s_wca);
-  bfree(s_alpha);
+  b->planned = false;  // shapes may have moved jobs between families
+  const cudaError_t e = restore();
   if (result != FW2V_OK) return result;
   BCK(b, e);
   if (report) *report = rep;

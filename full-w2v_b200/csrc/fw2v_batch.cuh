@@ -37,40 +37,56 @@ struct BatchTrainArgs {
   const float* exp_table;
 };
 
-// Stage counts compiled into the batched kernel (a job with 1 + K targets per
-// centre sweeps them in ceil((1 + K) / stages) groups).
+// Stage counts compiled into the batched kernels (a job with 1 + K targets
+// per centre sweeps them in ceil((1 + K) / stages) groups).
 constexpr int kBatchStages[] = {2, 3, 4, 6};
 
-template <typename T, int VEC, int R>
-__device__ __forceinline__ void batch_body(const TrainParams& p, const Sentence& sn, float* ring, T* orig,
-                                           const float* table, int lane) {
-  train_sentence<T, VEC, 1, R, 0>(p, sn, ring, orig, table, lane);
-}
+// Kernel families: rows of one vector per lane (d <= 128: 2-float lanes for
+// d <= 64, 4-float for d <= 128) within 128 registers and up to 16 warps per
+// SM; and wide rows of 2 or 3 four-float vectors per lane (d <= 384) with up
+// to 255 registers.
+constexpr int kBatchMaxWarps = 8;
+template <int FAMILY>
+struct BatchFamily;
+template <>
+struct BatchFamily<0> {
+  static constexpr int kMinBlocks = 2;
+};
+template <>
+struct BatchFamily<1> {
+  static constexpr int kMinBlocks = 1;
+};
 
-template <typename T>
-__device__ __forceinline__ void batch_dispatch(const TrainParams& p, const Sentence& sn, float* ring, T* orig,
-                                               const float* table, int lane) {
-  if (p.lane_vec == 2) {
-    switch (p.stages) {
-      case 2: batch_body<T, 2, 2>(p, sn, ring, orig, table, lane); break;
-      case 3: batch_body<T, 2, 3>(p, sn, ring, orig, table, lane); break;
-      case 4: batch_body<T, 2, 4>(p, sn, ring, orig, table, lane); break;
-      default: batch_body<T, 2, 6>(p, sn, ring, orig, table, lane); break;
-    }
-  } else {
-    switch (p.stages) {
-      case 2: batch_body<T, 4, 2>(p, sn, ring, orig, table, lane); break;
-      case 3: batch_body<T, 4, 3>(p, sn, ring, orig, table, lane); break;
-      case 4: batch_body<T, 4, 4>(p, sn, ring, orig, table, lane); break;
-      default: batch_body<T, 4, 6>(p, sn, ring, orig, table, lane); break;
-    }
+// Rows of three vectors per lane stop at 4 stages: their 6-stage body does not
+// fit the register file.
+template <typename T, int VEC, int NV>
+__device__ __forceinline__ void batch_stages(const TrainParams& p, const Sentence& sn, float* ring, T* orig,
+                                             const float* table, int lane) {
+  switch (p.stages) {
+    case 2: train_sentence<T, VEC, NV, 2, 0>(p, sn, ring, orig, table, lane); break;
+    case 3: train_sentence<T, VEC, NV, 3, 0>(p, sn, ring, orig, table, lane); break;
+    case 4: train_sentence<T, VEC, NV, 4, 0>(p, sn, ring, orig, table, lane); break;
+    default:
+      if constexpr (NV < 3) train_sentence<T, VEC, NV, 6, 0>(p, sn, ring, orig, table, lane);
+      break;
   }
 }
 
-constexpr int kBatchMaxWarps = 8;
+template <typename T, int FAMILY>
+__device__ __forceinline__ void batch_dispatch(const TrainParams& p, const Sentence& sn, float* ring, T* orig,
+                                               const float* table, int lane) {
+  if constexpr (FAMILY == 0) {
+    if (p.lane_vec == 2) batch_stages<T, 2, 1>(p, sn, ring, orig, table, lane);
+    else batch_stages<T, 4, 1>(p, sn, ring, orig, table, lane);
+  } else {
+    if (p.lane_nv == 2) batch_stages<T, 4, 2>(p, sn, ring, orig, table, lane);
+    else batch_stages<T, 4, 3>(p, sn, ring, orig, table, lane);
+  }
+}
 
-template <typename T>
-__global__ void __launch_bounds__(kBatchMaxWarps * 32, 2) sgns_batch_kernel(BatchTrainArgs a) {
+template <typename T, int FAMILY>
+__global__ void __launch_bounds__(kBatchMaxWarps * 32, BatchFamily<FAMILY>::kMinBlocks)
+    sgns_batch_kernel(BatchTrainArgs a) {
   extern __shared__ __align__(16) float smem[];
   __shared__ __align__(8) TrainParams tp[kBatchMaxWarps];
   const int lane = threadIdx.x & 31;
@@ -119,7 +135,7 @@ __global__ void __launch_bounds__(kBatchMaxWarps * 32, 2) sgns_batch_kernel(Batc
     sn.len = a.ent_len[slot];
     sn.alpha = a.ent_alpha[slot];
     sn.uid = a.uid_base[lo] + e;
-    batch_dispatch<T>(tp[warp], sn, ring, orig, a.exp_table, lane);
+    batch_dispatch<T, FAMILY>(tp[warp], sn, ring, orig, a.exp_table, lane);
   }
 }
 
@@ -127,10 +143,10 @@ __global__ void __launch_bounds__(kBatchMaxWarps * 32, 2) sgns_batch_kernel(Batc
 // by side in a block), as many blocks per SM as registers and shared memory
 // allow, at most `per_sm_cap` if that is positive, and no more warps than the
 // scratch covers.  Called before any stream capture.
-template <typename T>
+template <typename T, int FAMILY>
 cudaError_t batch_grid(int64_t smem_floats, int warps, int per_sm_cap, int num_sms, int64_t scratch_warps,
                        int deterministic, int* blocks, int* threads, size_t* smem) {
-  auto kern = sgns_batch_kernel<T>;
+  auto kern = sgns_batch_kernel<T, FAMILY>;
   if (deterministic) warps = 1;
   if (warps < 1 || warps > kBatchMaxWarps) return cudaErrorInvalidValue;
   *smem = (size_t)warps * (size_t)smem_floats * sizeof(float);
@@ -153,9 +169,9 @@ cudaError_t batch_grid(int64_t smem_floats, int warps, int per_sm_cap, int num_s
   return cudaSuccess;
 }
 
-template <typename T>
+template <typename T, int FAMILY>
 cudaError_t batch_launch(const BatchTrainArgs& a, int blocks, int threads, size_t smem, cudaStream_t st) {
-  sgns_batch_kernel<T><<<blocks, threads, smem, st>>>(a);
+  sgns_batch_kernel<T, FAMILY><<<blocks, threads, smem, st>>>(a);
   return cudaGetLastError();
 }
 

@@ -214,9 +214,9 @@ struct TrainParams {
   int64_t scratch_warps;
   uint64_t sr_seed;  // stochastic rounding of bfloat16 write-backs
   int bf16;          // tables hold bfloat16
-  // batched launches: lane vector width (2 or 4, one vector per lane) and
-  // pipeline stages of this job's sentences
-  int lane_vec, stages;
+  // batched launches: lane vector width (2 or 4), vectors per lane (1 to 3)
+  // and pipeline stages of this job's sentences
+  int lane_vec, lane_nv, stages;
 };
 
 // A round of a batched epoch: n sampling streams of any jobs.  Stream g of the

@@ -60,9 +60,10 @@ class BatchStats(C.Structure):
 
 class TuneReport(C.Structure):
     _fields_ = [("n_classes", C.c_int32), ("class_d", C.c_int32 * 16), ("class_window", C.c_int32 * 16),
-                ("class_lane_vec", C.c_int32 * 16), ("class_stages", C.c_int32 * 16),
-                ("tuned_wps", C.c_double * 16), ("default_wps", C.c_double * 16),
-                ("warps_per_block", C.c_int32), ("blocks_per_sm", C.c_int32)]
+                ("class_lane_vec", C.c_int32 * 16), ("class_lane_nv", C.c_int32 * 16),
+                ("class_stages", C.c_int32 * 16), ("tuned_wps", C.c_double * 16),
+                ("default_wps", C.c_double * 16), ("warps_per_block", C.c_int32 * 2),
+                ("blocks_per_sm", C.c_int32 * 2)]
 
 
 # Every entry point declared in include/fw2v.h (tests check the library exports them all).
@@ -132,10 +133,10 @@ def lib() -> C.CDLL:
             "fw2v_batch_last_error": (C.c_char_p, [H]),
             "fw2v_batch_add_job": (C.c_int, [H, C.POINTER(Config), P, I64, U64, P, I64, P, I64,
                                              C.POINTER(I32)]),
-            "fw2v_batch_set_shape": (C.c_int, [H, I32, I32, I32]),
-            "fw2v_batch_get_shape": (C.c_int, [H, I32, C.POINTER(I32), C.POINTER(I32)]),
-            "fw2v_batch_set_launch": (C.c_int, [H, I32, I32]),
-            "fw2v_batch_get_launch": (C.c_int, [H, C.POINTER(I32), C.POINTER(I32)]),
+            "fw2v_batch_set_shape": (C.c_int, [H, I32, I32, I32, I32]),
+            "fw2v_batch_get_shape": (C.c_int, [H, I32, C.POINTER(I32), C.POINTER(I32), C.POINTER(I32)]),
+            "fw2v_batch_set_launch": (C.c_int, [H, I32, I32, I32]),
+            "fw2v_batch_get_launch": (C.c_int, [H, I32, C.POINTER(I32), C.POINTER(I32)]),
             "fw2v_batch_tune": (C.c_int, [H, I64, C.POINTER(TuneReport)]),
             "fw2v_batch_train": (C.c_int, [H, C.POINTER(BatchStats)]),
             "fw2v_batch_job_words": (C.c_int, [H, I32, C.POINTER(U64), C.POINTER(U64)]),
@@ -340,7 +341,7 @@ class Trainer:
 class Batch:
     """Many independent SGNS jobs trained together on one GPU (a libfw2v
     batch): one persistent training kernel per round drains a work queue of
-    (job, sentence) items from every job.  Jobs need layer_size <= 128, the
+    (job, sentence) items from every job.  Jobs need layer_size <= 384, the
     table sigmoid and the same `negative`."""
 
     def __init__(self, precision: int = FP32, device: int = 0, use_graph: bool = True,
@@ -388,20 +389,22 @@ class Batch:
         self.jobs.append((config, len(counts)))
         return j.value
 
-    def set_shape(self, job: int, lane_vec: int, stages: int):
-        self._check(lib().fw2v_batch_set_shape(self._h, job, lane_vec, stages), "batch_set_shape")
+    def set_shape(self, job: int, lane_vec: int, lane_nv: int, stages: int):
+        self._check(lib().fw2v_batch_set_shape(self._h, job, lane_vec, lane_nv, stages), "batch_set_shape")
 
-    def shape(self, job: int) -> tuple[int, int]:
-        v, s = C.c_int32(), C.c_int32()
-        self._check(lib().fw2v_batch_get_shape(self._h, job, C.byref(v), C.byref(s)), "batch_get_shape")
-        return v.value, s.value
+    def shape(self, job: int) -> tuple[int, int, int]:
+        v, n, s = C.c_int32(), C.c_int32(), C.c_int32()
+        self._check(lib().fw2v_batch_get_shape(self._h, job, C.byref(v), C.byref(n), C.byref(s)),
+                    "batch_get_shape")
+        return v.value, n.value, s.value
 
-    def set_launch(self, warps_per_block: int, blocks_per_sm: int = 0):
-        self._check(lib().fw2v_batch_set_launch(self._h, warps_per_block, blocks_per_sm), "batch_set_launch")
+    def set_launch(self, family: int, warps_per_block: int, blocks_per_sm: int = 0):
+        self._check(lib().fw2v_batch_set_launch(self._h, family, warps_per_block, blocks_per_sm),
+                    "batch_set_launch")
 
-    def launch(self) -> tuple[int, int]:
+    def launch(self, family: int) -> tuple[int, int]:
         w, b = C.c_int32(), C.c_int32()
-        self._check(lib().fw2v_batch_get_launch(self._h, C.byref(w), C.byref(b)), "batch_get_launch")
+        self._check(lib().fw2v_batch_get_launch(self._h, family, C.byref(w), C.byref(b)), "batch_get_launch")
         return w.value, b.value
 
     def tune(self, sample_tokens: int = 0, cache: str | None = None) -> dict:
@@ -412,26 +415,30 @@ class Batch:
         import json
 
         keys = [self._class_key(c) for c, _ in self.jobs]
+        launch_keys = [f"launch{f}:{self._device_key()}" for f in (0, 1)]
         store = {}
         if cache and os.path.exists(cache):
             with open(cache) as f:
                 store = json.load(f)
-        if keys and all(k in store for k in keys) and "launch:" + self._device_key() in store:
+        if keys and all(k in store for k in keys + launch_keys):
             for j, k in enumerate(keys):
                 self.set_shape(j, *store[k])
-            self.set_launch(*store["launch:" + self._device_key()])
+            for f, k in enumerate(launch_keys):
+                self.set_launch(f, *store[k])
             return {"cached": True}
         rep = TuneReport()
         self._check(lib().fw2v_batch_tune(self._h, int(sample_tokens), C.byref(rep)), "batch_tune")
-        out = {"cached": False, "warps_per_block": rep.warps_per_block, "classes": []}
+        out = {"cached": False, "warps_per_block": list(rep.warps_per_block), "classes": []}
         for c in range(rep.n_classes):
             out["classes"].append({"d": rep.class_d[c], "window": rep.class_window[c],
-                                   "lane_vec": rep.class_lane_vec[c], "stages": rep.class_stages[c],
-                                   "tuned_wps": rep.tuned_wps[c], "default_wps": rep.default_wps[c]})
+                                   "lane_vec": rep.class_lane_vec[c], "lane_nv": rep.class_lane_nv[c],
+                                   "stages": rep.class_stages[c], "tuned_wps": rep.tuned_wps[c],
+                                   "default_wps": rep.default_wps[c]})
         if cache:
             for j, k in enumerate(keys):
                 store[k] = list(self.shape(j))
-            store["launch:" + self._device_key()] = list(self.launch())
+            for f, k in enumerate(launch_keys):
+                store[k] = list(self.launch(f))
             with open(cache, "w") as f:
                 json.dump(store, f, indent=1, sort_keys=True)
         return out
@@ -441,7 +448,8 @@ class Batch:
 
     def _class_key(self, c: Config) -> str:
         pitch = (c.layer_size + 7) // 8 * 8
-        return f"{self._device_key()}:d{'64' if pitch <= 64 else '128'}:w{c.window}:k{c.negative}"
+        cls = 64 if pitch <= 64 else 128 if pitch <= 128 else 256 if pitch <= 256 else 384
+        return f"{self._device_key()}:d{cls}:w{c.window}:k{c.negative}"
 
     def train(self) -> BatchStats:
         st = BatchStats()

@@ -247,9 +247,10 @@ const char* fw2v_version(void);
  * r+1 overlaps training of round r; with use_graph the whole call is captured
  * and replayed as one CUDA graph.
  *
- * Jobs: layer_size <= 128, sigmoid FW2V_SIGMOID_TABLE, the same `negative` in
+ * Jobs: layer_size <= 384, sigmoid FW2V_SIGMOID_TABLE, the same `negative` in
  * every job of a batch; the batch's precision and deterministic flags replace
- * the jobs' own. */
+ * the jobs' own.  Jobs with one vector per lane (d <= 128) and wide jobs (2 or
+ * 3 vectors per lane) run in separate rounds on two kernel families. */
 typedef struct fw2v_batch fw2v_batch;
 
 typedef struct fw2v_batch_config {
@@ -280,17 +281,21 @@ fw2v_status fw2v_batch_add_job(fw2v_batch* b, const fw2v_config* cfg, const uint
                                uint64_t train_words, const int32_t* stream, int64_t stream_len,
                                const int64_t* chunk_off, int64_t n_chunks, int32_t* job);
 
-/* A job's kernel shape: the lane vector width (2: 32 lanes of 2 floats cover
- * d <= 64; 4: lanes of 4 floats cover d <= 128, 16 lanes suffice for d <= 64)
- * and the pipeline stages (2, 3, 4 or 6 targets in flight).  Defaults follow
- * d and negative; fw2v_batch_tune picks them by measurement. */
-fw2v_status fw2v_batch_set_shape(fw2v_batch* b, int32_t job, int32_t lane_vec, int32_t stages);
-fw2v_status fw2v_batch_get_shape(fw2v_batch* b, int32_t job, int32_t* lane_vec, int32_t* stages);
+/* A job's kernel shape: the lane vector width and vectors per lane (2 x 1:
+ * 32 lanes of 2 floats cover d <= 64; 4 x 1: d <= 128, 16 lanes suffice for
+ * d <= 64; 4 x 2: d <= 256; 4 x 3: d <= 384) and the pipeline stages (2, 3, 4
+ * or 6 targets in flight).  Defaults follow d and negative; fw2v_batch_tune
+ * picks them by measurement. */
+fw2v_status fw2v_batch_set_shape(fw2v_batch* b, int32_t job, int32_t lane_vec, int32_t lane_nv, int32_t stages);
+fw2v_status fw2v_batch_get_shape(fw2v_batch* b, int32_t job, int32_t* lane_vec, int32_t* lane_nv,
+                                 int32_t* stages);
 
-/* The training grid: warps per block (sentences trained side by side in one
- * block, 1..8) and a cap on blocks per SM (0: as many as fit). */
-fw2v_status fw2v_batch_set_launch(fw2v_batch* b, int32_t warps_per_block, int32_t blocks_per_sm);
-fw2v_status fw2v_batch_get_launch(fw2v_batch* b, int32_t* warps_per_block, int32_t* blocks_per_sm);
+/* The training grid of a kernel family (0: one vector per lane, 1: wide
+ * rows): warps per block (sentences trained side by side in one block, 1..8)
+ * and a cap on blocks per SM (0: as many as fit). */
+fw2v_status fw2v_batch_set_launch(fw2v_batch* b, int32_t family, int32_t warps_per_block, int32_t blocks_per_sm);
+fw2v_status fw2v_batch_get_launch(fw2v_batch* b, int32_t family, int32_t* warps_per_block,
+                                  int32_t* blocks_per_sm);
 
 /* Autotuner: for every class of jobs with the same (lane-vector class of d,
  * window), time every shape on a sample of up to sample_tokens of the class's
@@ -300,9 +305,9 @@ fw2v_status fw2v_batch_get_launch(fw2v_batch* b, int32_t* warps_per_block, int32
  * words/s (tuned_wps) and the default shape's (default_wps), n_classes. */
 typedef struct fw2v_batch_tune_report {
   int32_t n_classes;
-  int32_t class_d[16], class_window[16], class_lane_vec[16], class_stages[16];
+  int32_t class_d[16], class_window[16], class_lane_vec[16], class_lane_nv[16], class_stages[16];
   double tuned_wps[16], default_wps[16];
-  int32_t warps_per_block, blocks_per_sm;
+  int32_t warps_per_block[2], blocks_per_sm[2];  /* per kernel family */
 } fw2v_batch_tune_report;
 fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2v_batch_tune_report* report);
 

@@ -50,6 +50,9 @@ def _jobs():
         (_walk_corpus(), dict(layer_size=100, window=5, threads=3, msl=1000, epochs=1, sample=1e-3, seed=11)),
         (_golden_corpus("zipf_t3", 40), dict(layer_size=128, window=2, threads=3, msl=40, epochs=3, sample=1e-3,
                                               seed=5)),
+        (_golden_corpus("eos_t1", 60), dict(layer_size=200, window=2, threads=1, msl=60, epochs=2, sample=1e-4,
+                                             seed=17)),
+        (_walk_corpus(), dict(layer_size=300, window=4, threads=2, msl=1000, epochs=1, sample=1e-3, seed=23)),
     ]
 
 
@@ -57,9 +60,10 @@ def _config(over):
     return fw2v.default_config(negative=K, alpha=0.025, **over)
 
 
-def _oracle_job(corpus, over, lane_vec, bf16=False):
+def _oracle_job(corpus, over, shape, bf16=False):
     """The job alone on the oracle: (syn0, syn1neg) as float32 arrays [V, d]."""
     d, W, E, seed = over["layer_size"], over["window"], over["epochs"], over["seed"]
+    lane_vec, lane_nv = shape[0], shape[1]
     V = len(corpus.counts)
     out = O.sample_streams(corpus, threads=over["threads"], msl=over["msl"], negative=K, epochs=E, alpha0=0.025,
                            sample=over["sample"], seed=seed)
@@ -75,10 +79,10 @@ def _oracle_job(corpus, over, lane_vec, bf16=False):
         if bf16:
             sr = O.mix64((0x5EEDF00D + e + O.seed_offset(seed)) & MASK)
             O.train_bf16(syn0, syn1, lens, alphas, ids, negs, d=d, window=W, negative=K, seed=sr, sigmoid="table",
-                         vec=lane_vec, nv=1)
+                         vec=lane_vec, nv=lane_nv)
         else:
             O.train(syn0, syn1, lens, alphas, ids, negs, d=d, window=W, negative=K, sigmoid="table", precision=32,
-                    vec=lane_vec, nv=1)
+                    vec=lane_vec, nv=lane_nv)
     if bf16:
         return O.bf16_float(syn0), O.bf16_float(syn1)
     return syn0, syn1
@@ -108,8 +112,7 @@ def test_deterministic_batch_equals_each_job_alone_fp32(jobs, use_graph):
         st = b.train()
         assert st.rounds > 3 and st.epochs == 3
         for j, (corpus, over) in enumerate(jobs):
-            lane_vec, stages = b.shape(j)
-            r0, r1 = _oracle_job(corpus, over, lane_vec)
+            r0, r1 = _oracle_job(corpus, over, b.shape(j))
             np.testing.assert_array_equal(b.syn0(j), r0[:, :over["layer_size"]])
             np.testing.assert_array_equal(b.syn1neg(j), r1[:, :over["layer_size"]])
             assert b.job_words(j)[0] == _words(corpus, over)
@@ -119,18 +122,22 @@ def test_deterministic_batch_equals_each_job_alone_bf16(jobs):
     with _batch(jobs, precision=fw2v.BF16, deterministic=True, round_tokens=5000) as b:
         b.train()
         for j, (corpus, over) in enumerate(jobs):
-            r0, r1 = _oracle_job(corpus, over, b.shape(j)[0], bf16=True)
+            r0, r1 = _oracle_job(corpus, over, b.shape(j), bf16=True)
             np.testing.assert_array_equal(b.syn0(j), r0[:, :over["layer_size"]])
             np.testing.assert_array_equal(b.syn1neg(j), r1[:, :over["layer_size"]])
 
 
-@pytest.mark.parametrize("lane_vec,stages", [(2, 2), (2, 3), (2, 4), (2, 6), (4, 2), (4, 3), (4, 4), (4, 6)])
-def test_every_shape_trains_bit_exact(jobs, lane_vec, stages):
-    corpus, over = jobs[2]  # d = 64, window 10: every shape applies
+SHAPES = ([(2, (2, 1, s)) for s in (2, 3, 4, 6)] + [(2, (4, 1, s)) for s in (2, 3, 4, 6)] +
+          [(5, (4, 2, s)) for s in (2, 3, 4, 6)] + [(6, (4, 3, s)) for s in (2, 3, 4)])
+
+
+@pytest.mark.parametrize("job,shape", SHAPES)
+def test_every_shape_trains_bit_exact(jobs, job, shape):
+    corpus, over = jobs[job]  # d = 64 (one-vector layouts), 200 and 300 (wide rows)
     with _batch([(corpus, over)], deterministic=True) as b:
-        b.set_shape(0, lane_vec, stages)
+        b.set_shape(0, *shape)
         b.train()
-        r0, r1 = _oracle_job(corpus, over, lane_vec)
+        r0, r1 = _oracle_job(corpus, over, shape)
         np.testing.assert_array_equal(b.syn0(0), r0)
         np.testing.assert_array_equal(b.syn1neg(0), r1)
 
@@ -138,7 +145,7 @@ def test_every_shape_trains_bit_exact(jobs, lane_vec, stages):
 def test_batch_job_equals_single_job_handle(jobs):
     corpus, over = jobs[3]
     with _batch([(corpus, over)], deterministic=True) as b:
-        b.set_shape(0, 4, 6)
+        b.set_shape(0, 4, 1, 6)  # the single-job kernel's layout for d = 100 and negative 5
         b.train()
         got0, got1 = b.syn0(0), b.syn1neg(0)
     with fw2v.Trainer(_config(dict(over, deterministic=1))) as t:
@@ -184,8 +191,8 @@ def test_tuner_picks_valid_shapes_and_restores_state(jobs):
         assert rep["classes"] and all(c["tuned_wps"] >= c["default_wps"] > 0 for c in rep["classes"])
         for j, (corpus, over) in enumerate(jobs):
             np.testing.assert_array_equal(b.syn0(j), before[j])
-            vec, st = b.shape(j)
-            assert st in (2, 3, 4, 6) and vec * 32 >= over["layer_size"]
+            vec, nv, st = b.shape(j)
+            assert st in (2, 3, 4, 6) and vec * nv * 32 >= over["layer_size"]
         st = b.train()  # sampler state was restored: the same words as never tuned
         assert st.words_read == sum(_words(c, o) for c, o in jobs)
 
@@ -205,14 +212,15 @@ def test_batch_rejects_bad_jobs(jobs):
     corpus, over = jobs[0]
     with fw2v.Batch() as b:
         with pytest.raises(fw2v.Fw2vError):
-            b.add_job(_config(dict(over, layer_size=200)), corpus.counts, corpus.train_words, corpus.stream,
+            b.add_job(_config(dict(over, layer_size=400)), corpus.counts, corpus.train_words, corpus.stream,
                       corpus.chunk_off)
         b.add_job(_config(over), corpus.counts, corpus.train_words, corpus.stream, corpus.chunk_off)
         with pytest.raises(fw2v.Fw2vError):
             b.add_job(fw2v.default_config(negative=3, **{k: v for k, v in over.items()}), corpus.counts,
                       corpus.train_words, corpus.stream, corpus.chunk_off)
-        with pytest.raises(fw2v.Fw2vError):
-            b.set_shape(0, 2, 5)
+        for bad_shape in ((2, 1, 5), (4, 2, 6), (2, 2, 4)):  # no such stages; d = 8 needs one vector; 2-float wide
+            with pytest.raises(fw2v.Fw2vError):
+                b.set_shape(0, *bad_shape)
         bad = corpus.stream.copy()
         bad[3] = len(corpus.counts) + 7
         with pytest.raises(fw2v.Fw2vError):
