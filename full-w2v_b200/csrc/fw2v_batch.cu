@@ -70,7 +70,6 @@ struct BatchJob {
   std::vector<int64_t> sbase;  // threads + 1: readable-token prefix of its streams
   int64_t gfirst = 0;          // global number of its stream 0
   int lane_vec = 4, lane_nv = 1, stages = 6;
-  uint64_t epochs_done = 0;
   int family() const { return lane_nv >= 2 ? 1 : 0; }
 };
 
@@ -169,6 +168,7 @@ struct fw2v_batch {
   void* orig_scratch = nullptr;
   int64_t scratch_elems = 0, scratch_warps = 0, scratch_bytes = 0;
   int warps_per_block[2] = {4, 4}, blocks_per_sm[2] = {0, 0};  // per kernel family
+  int epochs_run = 0;  // batch epochs trained so far: job j has trained min(epochs_run, its epochs)
 };
 
 namespace {
@@ -279,8 +279,8 @@ SamplerParams sampler_params(const fw2v_batch* b, const BatchJob& j, const Round
   return p;
 }
 
-// sr_seed holds the job's base: the kernel adds the epoch and mixes (the
-// single-job seed of the same launch number).
+// sr_seed holds the job's seed offset: the kernel adds the (absolute) epoch
+// and mixes, which is the single-job seed of the same launch number.
 TrainParams train_params(const fw2v_batch* b, const BatchJob& j, const RoundBuf& rb) {
   TrainParams p{};
   p.syn0 = j.syn0;
@@ -297,7 +297,7 @@ TrainParams train_params(const fw2v_batch* b, const BatchJob& j, const RoundBuf&
   p.deterministic = b->cfg.deterministic;
   p.error_flag = b->error_flag;
   p.exp_table = b->exp_table;
-  p.sr_seed = j.soff + j.epochs_done;
+  p.sr_seed = j.soff;
   p.bf16 = b->elem == 2;
   p.lane_vec = j.lane_vec;
   p.lane_nv = j.lane_nv;
@@ -477,13 +477,14 @@ cudaError_t enqueue_sample(fw2v_batch* b, RoundBuf& rb, const BatchRound& r, int
                               rb.entry_prefix, b->sst);
 }
 
-// Every round of `epochs` epochs: sampler stream and training stream joined
-// by events, ending with the sampler stream joined into the training stream.
-cudaError_t enqueue_epochs(fw2v_batch* b, int epochs, const Grid* grids) {
+// Every round of epochs [e0, e0 + epochs): sampler stream and training stream
+// joined by events, ending with the sampler stream joined into the training
+// stream.  Jobs past their own epoch count sample nothing in an epoch.
+cudaError_t enqueue_epochs(fw2v_batch* b, int e0, int epochs, const Grid* grids) {
   cudaError_t e = cudaEventRecord(b->ev_fork, b->st);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(b->sst, b->ev_fork, 0);
   int64_t k = 0;
-  for (int ep = 0; ep < epochs && e == cudaSuccess; ep++) {
+  for (int ep = e0; ep < e0 + epochs && e == cudaSuccess; ep++) {
     e = cudaMemsetAsync(b->job_uid, 0, b->jobs.size() * sizeof(int64_t), b->sst);
     for (size_t ri = 0; ri < b->rounds.size() && e == cudaSuccess; ri++, k++) {
       RoundBuf& rb = b->buf[k % 2];
@@ -771,8 +772,8 @@ fw2v_status fw2v_batch_get_launch(fw2v_batch* b, int32_t family, int32_t* warps_
   return FW2V_OK;
 }
 
-fw2v_status fw2v_batch_train(fw2v_batch* b, fw2v_batch_stats* stats) {
-  if (!b) return FW2V_ERR_ARGUMENT;
+fw2v_status fw2v_batch_train_epochs(fw2v_batch* b, int32_t n_epochs, fw2v_batch_stats* stats) {
+  if (!b || n_epochs < 0) return bfail(b, FW2V_ERR_ARGUMENT, "epochs >= 0");
   BCK(b, cudaSetDevice(b->cfg.device));
   fw2v_status s = plan(b);
   if (s != FW2V_OK) return s;
@@ -785,8 +786,14 @@ fw2v_status fw2v_batch_train(fw2v_batch* b, fw2v_batch_stats* stats) {
     s = grid_for(b, all, fam, b->warps_per_block[fam], b->blocks_per_sm[fam], &g[fam]);
     if (s != FW2V_OK) return s;
   }
-  int epochs = 0;
-  for (const BatchJob& j : b->jobs) epochs = std::max(epochs, j.cfg.epochs);
+  int max_epochs = 0;
+  for (const BatchJob& j : b->jobs) max_epochs = std::max(max_epochs, j.cfg.epochs);
+  const int e0 = b->epochs_run;
+  const int epochs = std::min(n_epochs, std::max(0, max_epochs - e0));
+  if (epochs == 0) {
+    if (stats) *stats = fw2v_batch_stats{};
+    return FW2V_OK;
+  }
   const size_t J = b->jobs.size();
   BCK(b, cudaMemsetAsync(b->job_words, 0, J * sizeof(unsigned long long), b->st));
   BCK(b, cudaMemsetAsync(b->job_kept, 0, J * sizeof(unsigned long long), b->st));
@@ -796,7 +803,7 @@ fw2v_status fw2v_batch_train(fw2v_batch* b, fw2v_batch_stats* stats) {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     BCK(b, cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
-    const cudaError_t e = enqueue_epochs(b, epochs, g);
+    const cudaError_t e = enqueue_epochs(b, e0, epochs, g);
     const cudaError_t e2 = cudaStreamEndCapture(b->st, &graph);
     BCK(b, e);
     BCK(b, e2);
@@ -808,7 +815,7 @@ fw2v_status fw2v_batch_train(fw2v_batch* b, fw2v_batch_stats* stats) {
     cudaGraphDestroy(graph);
     BCK(b, e3);
   } else {
-    BCK(b, enqueue_epochs(b, epochs, g));
+    BCK(b, enqueue_epochs(b, e0, epochs, g));
     BCK(b, cudaEventRecord(b->ev_end, b->st));
     BCK(b, cudaStreamSynchronize(b->st));
   }
@@ -823,13 +830,17 @@ fw2v_status fw2v_batch_train(fw2v_batch* b, fw2v_batch_stats* stats) {
     b->kept_total[i] += k[i];
     out.words_read += w[i];
     out.words_kept += k[i];
-    b->jobs[i].epochs_done += (uint64_t)b->jobs[i].cfg.epochs;
   }
+  b->epochs_run += epochs;
   BCK(b, cudaEventElapsedTime(&out.ms, b->ev_start, b->ev_end));
   out.epochs = epochs;
   out.rounds = (int32_t)b->rounds.size();
   if (stats) *stats = out;
   return FW2V_OK;
+}
+
+fw2v_status fw2v_batch_train(fw2v_batch* b, fw2v_batch_stats* stats) {
+  return fw2v_batch_train_epochs(b, INT32_MAX, stats);
 }
 
 }  // extern "C"

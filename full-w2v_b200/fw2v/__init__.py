@@ -77,7 +77,8 @@ EXPORTS = [
     "fw2v_kernel_batch_noalloc", "fw2v_reorder_chunks",
     "fw2v_batch_config_default", "fw2v_batch_create", "fw2v_batch_destroy", "fw2v_batch_last_error",
     "fw2v_batch_add_job", "fw2v_batch_set_shape", "fw2v_batch_get_shape", "fw2v_batch_set_launch",
-    "fw2v_batch_get_launch", "fw2v_batch_tune", "fw2v_batch_train", "fw2v_batch_job_words",
+    "fw2v_batch_get_launch", "fw2v_batch_tune", "fw2v_batch_train", "fw2v_batch_train_epochs",
+    "fw2v_batch_job_words",
     "fw2v_batch_get_syn0", "fw2v_batch_get_syn1neg",
 ]
 
@@ -139,6 +140,7 @@ def lib() -> C.CDLL:
             "fw2v_batch_get_launch": (C.c_int, [H, I32, C.POINTER(I32), C.POINTER(I32)]),
             "fw2v_batch_tune": (C.c_int, [H, I64, C.POINTER(TuneReport)]),
             "fw2v_batch_train": (C.c_int, [H, C.POINTER(BatchStats)]),
+            "fw2v_batch_train_epochs": (C.c_int, [H, I32, C.POINTER(BatchStats)]),
             "fw2v_batch_job_words": (C.c_int, [H, I32, C.POINTER(U64), C.POINTER(U64)]),
             "fw2v_batch_get_syn0": (C.c_int, [H, I32, P, I64]),
             "fw2v_batch_get_syn1neg": (C.c_int, [H, I32, P, I64]),
@@ -452,8 +454,15 @@ class Batch:
         return f"{self._device_key()}:d{cls}:w{c.window}:k{c.negative}"
 
     def train(self) -> BatchStats:
+        """Every job's remaining epochs."""
         st = BatchStats()
         self._check(lib().fw2v_batch_train(self._h, C.byref(st)), "batch_train")
+        return st
+
+    def train_epochs(self, n: int) -> BatchStats:
+        """The next n epochs of every job that has epochs left."""
+        st = BatchStats()
+        self._check(lib().fw2v_batch_train_epochs(self._h, n, C.byref(st)), "batch_train_epochs")
         return st
 
     def job_words(self, job: int) -> tuple[int, int]:

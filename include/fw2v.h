@@ -311,8 +311,13 @@ typedef struct fw2v_batch_tune_report {
 } fw2v_batch_tune_report;
 fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2v_batch_tune_report* report);
 
-/* Train every job for its configured epochs (from the current state). */
+/* Train every job until it has trained its configured epochs (as fw2v_train:
+ * a second call trains nothing). */
 fw2v_status fw2v_batch_train(fw2v_batch* b, fw2v_batch_stats* stats);
+
+/* Train the next n_epochs epochs of every job that has epochs left (as that
+ * many fw2v_train_epoch calls); with use_graph, as one graph. */
+fw2v_status fw2v_batch_train_epochs(fw2v_batch* b, int32_t n_epochs, fw2v_batch_stats* stats);
 
 /* Words read and kept by one job since it was added. */
 fw2v_status fw2v_batch_job_words(fw2v_batch* b, int32_t job, uint64_t* words_read, uint64_t* words_kept);

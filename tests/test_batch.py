@@ -156,12 +156,15 @@ def test_batch_job_equals_single_job_handle(jobs):
         np.testing.assert_array_equal(t.syn1neg(), got1)
 
 
-def test_second_train_call_continues_like_a_single_job(jobs):
-    """Two calls: epochs continue the LCG streams and the rounding seeds."""
-    corpus, over = jobs[0]
+def test_epochs_one_call_at_a_time_continue_like_a_single_job(jobs):
+    """Epoch by epoch: the LCG streams, learning rates and rounding seeds
+    continue across calls, and a call after the last epoch trains nothing."""
+    corpus, over = jobs[4]  # three epochs
     with _batch([(corpus, over)], precision=fw2v.BF16, deterministic=True) as b:
-        b.train()
-        b.train()
+        assert b.train_epochs(1).epochs == 1
+        assert b.train_epochs(1).epochs == 1
+        assert b.train().epochs == 1
+        assert b.train().words_read == 0
         got = b.syn0(0)
     with fw2v.Trainer(_config(dict(over, deterministic=1, precision=fw2v.BF16))) as t:
         t.set_vocab(corpus.counts, corpus.train_words)
