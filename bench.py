@@ -186,118 +186,225 @@ def cpu_baseline(corpus, cfg, threads, seconds_target=15.0):
                       f"FP32 Hogwild on {cores} threads"}
 
 
+def make_corpus(args):
+    """(corpus, held-out stream or None, config) of the workload: the numpy
+    generator for c1/c2 (the reference program reads the same corpus as text),
+    the device generator for c3 (800M tokens)."""
+    from fw2v import synth
+    if args.config == "c3":
+        return synth.make_topic_corpus_gpu(args.config, n_tokens=args.tokens, heldout_tokens=args.heldout)
+    corpus, cfg = synth.make_topic_corpus(args.config, n_tokens=args.tokens)
+    return corpus, None, cfg
+
+
+def job_config(args, cfg, T, epochs, precision):
+    import fw2v
+    return fw2v.default_config(layer_size=cfg["d"], window=cfg["window"], negative=cfg["negative"], epochs=epochs,
+                               threads=T, msl=1000, alpha=0.025, sample=cfg["sample"], precision=precision)
+
+
+def timed_epochs(args, world, dev, run_epoch, flush, stream):
+    """W untimed epochs, then K timed ones bracketed by barrier + synchronize;
+    run_epoch() -> (words read, words kept, device ms, kernel launches)."""
+    import torch
+    for _ in range(args.warmup):
+        run_epoch()
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    res = []
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(i & 0xFF)  # L2 flush, not timed
+        torch.cuda.synchronize(dev)
+        res.append(run_epoch())
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    return res
+
+
+def heldout(tr_cls, corpus, cfg, pairs, syn0, syn1):
+    """Mean held-out SGNS loss per pair of tables (FP32 evaluation of the values)."""
+    import fw2v
+    from fw2v import evaluate
+    c = fw2v.default_config(layer_size=cfg["d"], window=cfg["window"], negative=cfg["negative"], epochs=1,
+                            threads=1, msl=1000, sample=0.0)
+    with tr_cls(c) as t:
+        t.set_vocab(corpus.counts, corpus.train_words)
+        t.set_tables(syn0, syn1)
+        return evaluate.heldout_loss(t, pairs)
+
+
 def run_own(args, world, rank, local):
     import torch
 
     import fw2v
-    from fw2v import synth
+    from fw2v import evaluate
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    corpus, cfg = synth.make_topic_corpus(args.config, n_tokens=args.tokens)
+    corpus, held, cfg = make_corpus(args)
     T = args.streams or default_streams(len(corpus.chunk_off))
     d, W, K = cfg["d"], cfg["window"], cfg["negative"]
     epochs = args.warmup + args.steps
-    conf = fw2v.default_config(layer_size=d, window=W, negative=K, epochs=epochs, threads=T,
-                               msl=1000, alpha=0.025, sample=cfg["sample"],
-                               precision=fw2v.BF16 if args.precision == "bf16" else fw2v.FP32,
-                               device=local)
-    tr = fw2v.Trainer(conf)
-    tr.set_vocab(corpus.counts, corpus.train_words)
-    tr.load_corpus(corpus.stream, corpus.chunk_off)
-    stream = torch.cuda.ExternalStream(tr.stream_handle(), device=dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    form = args.form
+    bf16 = form.startswith("bf16")
+    prec = fw2v.BF16 if bf16 else fw2v.FP32
+    pairs = None
+    if held is not None and len(held) > 0:
+        pairs = evaluate.heldout_pairs(corpus.counts, corpus.train_words, held, window=W, negative=K)
+    tune_cache = os.path.join(tempfile.mkdtemp(prefix="fw2v_tune_"), "tune.json")
+    tuned = None
 
-    for _ in range(args.warmup):
-        tr.train_epoch()
-    barrier(world)
-    torch.cuda.synchronize(dev)
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    stats = []
     with ClockSampler(local) as clk:
-        for i in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(i & 0xFF)
-            starts[i].record(stream)
-            stats.append(tr.train_epoch())
-            ends[i].record(stream)
-        torch.cuda.synchronize(dev)
-    barrier(world)
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_s = max_over_ranks(world, sum(step_ms) / 1e3)
-    words = sum(s.words_read for s in stats)
-    kept = sum(s.words_kept for s in stats)
-    words_all = sum_over_ranks(world, float(words))
-    value = words_all / total_s
-    train_ms = float(np.mean([s.train_ms for s in stats]))
-    sampler_ms = float(np.mean([s.sampler_ms for s in stats]))
+        if form.endswith("batched"):
+            b = fw2v.Batch(precision=prec, device=local)
+            b.add_job(job_config(args, cfg, T, epochs, prec), corpus.counts, corpus.train_words, corpus.stream,
+                      corpus.chunk_off)
+            tuned = b.tune(cache=tune_cache)
 
-    # e2e: host buffers through the public API every step
+            def run_epoch():
+                # per round: sampler, negatives, entry prefix, job bookkeeping, trainer
+                st = b.train_epochs(1)
+                return st.words_read, st.words_kept, st.ms, 5 * st.rounds
+
+            res = timed_epochs(args, world, dev, run_epoch, flush, stream)
+            syn0, syn1 = b.syn0(0), b.syn1neg(0)
+            shape = b.shape(0)
+            b.close()
+        else:
+            tr = fw2v.Trainer(job_config(args, cfg, T, epochs, prec))
+            tr.set_vocab(corpus.counts, corpus.train_words)
+            tr.load_corpus(corpus.stream, corpus.chunk_off)
+            tstream = torch.cuda.ExternalStream(tr.stream_handle(), device=dev)
+
+            # device time of an epoch: events on the trainer's stream around it;
+            # per epoch: sampler, negatives, entry prefix, trainer
+            def run_epoch_timed():
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(tstream)
+                st = tr.train_epoch()
+                e1.record(tstream)
+                e1.synchronize()
+                return st.words_read, st.words_kept, e0.elapsed_time(e1), 4
+
+            res = timed_epochs(args, world, dev, run_epoch_timed, flush, stream)
+            syn0, syn1 = tr.syn0(), tr.syn1neg()
+            shape = None
+            tr.close()
+    words = sum(r[0] for r in res)
+    kept = sum(r[1] for r in res)
+    total_s = max_over_ranks(world, sum(r[2] for r in res) / 1e3)
+    value = sum_over_ranks(world, float(words)) / total_s
+    loss = heldout(fw2v.Trainer, corpus, cfg, pairs, syn0, syn1) if pairs is not None else None
+    del syn0, syn1
+
+    # e2e: through the public API from pinned host buffers, every step
     pinned = torch.empty(len(corpus.stream), dtype=torch.int32, pin_memory=True)
     pinned.numpy()[:] = corpus.stream
     host_stream = pinned.numpy()
-    e2e_steps = max(1, min(args.steps, 3))
-    e2e_words = 0
-    e2e_s = 0.0
+    e2e_steps = max(1, min(args.steps, 2))
+    e2e_words, e2e_s = 0, 0.0
     for i in range(e2e_steps):
         with torch.cuda.stream(stream):
             flush.fill_(i & 0xFF)
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        tr.load_corpus(host_stream, corpus.chunk_off)
-        tr.sample_epoch()
-        st = tr.train_sampled()
-        e2e_words += st.words_read
+        if form.endswith("batched"):
+            with fw2v.Batch(precision=prec, device=local) as eb:
+                eb.add_job(job_config(args, cfg, T, 1, prec), corpus.counts, corpus.train_words, host_stream,
+                           corpus.chunk_off)
+                eb.tune(cache=tune_cache)  # the shapes chosen above, from the cache
+                st = eb.train_epochs(1)
+                e2e_words += st.words_read
+        else:
+            with fw2v.Trainer(job_config(args, cfg, T, 1, prec)) as et:
+                et.set_vocab(corpus.counts, corpus.train_words)
+                et.load_corpus(host_stream, corpus.chunk_off)
+                et.sample_epoch()
+                e2e_words += et.train_sampled().words_read
         e2e_s += time.perf_counter() - t0
     e2e_s = max_over_ranks(world, e2e_s)
     e2e_value = sum_over_ranks(world, float(e2e_words)) / e2e_s
-    h2d = corpus.stream.nbytes + corpus.chunk_off.nbytes
-    d2h = T * 8 + 4
+    h2d = corpus.stream.nbytes + corpus.chunk_off.nbytes + corpus.counts.nbytes
+    d2h = 8 * T + 16
+
+    # the plain FP32 kernel on the same workload, for the form's speed-up
+    compare = None
+    if form != "fp32" and not args.no_compare:
+        tr = fw2v.Trainer(job_config(args, cfg, T, 1 + min(args.steps, 2), fw2v.FP32))
+        tr.set_vocab(corpus.counts, corpus.train_words)
+        tr.load_corpus(corpus.stream, corpus.chunk_off)
+        tstream = torch.cuda.ExternalStream(tr.stream_handle(), device=dev)
+        tr.train_epoch()
+        ms, cw = 0.0, 0
+        for i in range(min(args.steps, 2)):
+            with torch.cuda.stream(stream):
+                flush.fill_(i & 0xFF)
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(tstream)
+            cw += tr.train_epoch().words_read
+            e1.record(tstream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+        cval = sum_over_ranks(world, float(cw)) / max_over_ranks(world, ms / 1e3)
+        closs = heldout(fw2v.Trainer, corpus, cfg, pairs, tr.syn0(), tr.syn1neg()) if pairs is not None else None
+        tr.close()
+        compare = {"form": "fp32 (single-job kernel, untuned)", "value": cval, "unit": UNIT,
+                   "epochs_timed": min(args.steps, 2), "heldout_loss": closs,
+                   "speedup": value / cval,
+                   "heldout_loss_rel_diff": (loss - closs) / closs if loss is not None and closs else None}
 
     hbm, peak_kind = peaks()
+    elem = 2 if bf16 else 4
     kept_per_epoch = kept / args.steps
-    bytes_per_launch = kept_per_epoch * (2 * d * 4 * (K + 2) + 4 * (1 + K))
-    achieved = bytes_per_launch / (train_ms / 1e3) / 1e9
+    epoch_ms = total_s * 1e3 / args.steps
+    bytes_per_epoch = kept_per_epoch * (2 * d * elem * (K + 2) + 4 * (1 + K))
+    achieved = bytes_per_epoch / (epoch_ms / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
             tr_map = json.load(f)
-        key = f"{args.config}:{args.tokens or cfg['n_tokens']}:{args.precision}"
+        key = f"{args.config}:{args.tokens or cfg['n_tokens']}:{form}"
         if key in tr_map:
             traffic = tr_map[key]["dram_bytes_per_launch"]
-
+    kernel = "sgns_batch_kernel" if form.endswith("batched") else "sgns_train_kernel"
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps,
+        "warmup": args.warmup, "ms_per_step": epoch_ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32" if args.precision == "fp32" else "bf16-tables/f32-math",
+        "dtype": "bf16-tables/f32-math" if bf16 else "f32",
         "data": "synthetic (seeded topic-mixture corpus, generated in-process)",
-        "config": {"workload": f"{args.config}: {cfg['n_tokens']/1e6:.0f}M-token topic corpus, "
-                               f"V={len(corpus.counts)}, d={d}, window={W}, negative={K}, "
-                               f"sample={cfg['sample']}, msl=1000, {T} sampling streams, "
-                               f"{args.precision} tables",
-                   "tokens_per_epoch": int(len(corpus.stream) - 1), "vocab": len(corpus.counts),
-                   "layer_size": d, "window": W, "negative": K, "streams": T,
+        "config": {"workload": f"{args.config}: {(args.tokens or cfg['n_tokens'])/1e6:.0f}M-token topic corpus, "
+                               f"V={len(corpus.counts)}, d={d}, window={W}, negative={K}, sample={cfg['sample']}, "
+                               f"msl=1000, {T} sampling streams; form {form}",
+                   "form": form, "tokens_per_epoch": int(len(corpus.stream) - 1), "vocab": len(corpus.counts),
+                   "layer_size": d, "window": W, "negative": K, "streams": T, "shape": shape,
+                   "tuning": tuned,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": "flushed between steps (256 MB write, untimed)"},
+                   "l2": "flushed between steps (256 MB write, untimed); tables exceed L2"
+                         if args.config == "c3" else "flushed between steps (256 MB write, untimed)"},
+        "heldout_loss": loss,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
-        "gpu_launches": 4 * args.steps,
+        "gpu_launches": int(sum(r[3] for r in res)),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": traffic,
-                     "kernel": "sgns_train_kernel", "peak_kind": peak_kind,
-                     "bytes_per_launch": bytes_per_launch, "launch_ms": train_ms},
-        "breakdown": {"sampler_ms": sampler_ms, "train_ms": train_ms,
-                      "kept_fraction": kept / max(words, 1)},
+                     "frac": achieved / hbm, "traffic": traffic, "kernel": kernel, "peak_kind": peak_kind,
+                     "bytes_per_launch": bytes_per_epoch, "launch_ms": epoch_ms,
+                     "note": "algorithmic bytes of one epoch (rows of 1+K targets and one context per kept "
+                             "word, read and written, plus its ids) over the epoch's device time"},
+        "breakdown": {"kept_fraction": kept / max(words, 1)},
     }
+    if compare is not None:
+        out["fp32_plain"] = compare
     clocks = clk.summary()
     if clocks:
         out["clocks"] = clocks
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(corpus, cfg, T)
-    tr.close()
     return out
 
 
@@ -309,7 +416,7 @@ def run_reference(args, world, rank):
 
     if world > 1 and rank != 0:
         return None
-    corpus, cfg = synth.make_topic_corpus(args.config, n_tokens=args.tokens)
+    corpus, _, cfg = make_corpus(args)
     T_stream = args.streams or default_streams(len(corpus.chunk_off))
     cores = os.cpu_count() or 1
     binary = os.path.join(ROOT, "oracle", "_ref", "FULL-W2V")
@@ -412,10 +519,14 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fw2v", choices=["fw2v", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3"])
     ap.add_argument("--tokens", type=int, default=None, help="override the corpus size")
     ap.add_argument("--streams", type=int, default=None, help="sampling streams (-threads)")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16"])
+    ap.add_argument("--form", default="bf16-batched", choices=["bf16-batched", "fp32-batched", "bf16", "fp32"],
+                    help="tables and kernel: batched (persistent multi-job kernel, tuned, CUDA graph) or the "
+                         "single-job kernel")
+    ap.add_argument("--heldout", type=int, default=1_000_000, help="held-out tokens (c3)")
+    ap.add_argument("--no-compare", action="store_true", help="skip the plain FP32 comparison run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     world, rank, local = dist_setup()

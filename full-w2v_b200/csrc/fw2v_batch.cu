@@ -39,14 +39,16 @@ cudaError_t launch_sampler_round(const SamplerParams* d_jobs, const BatchRound& 
                                  const uint64_t* words, int n_jobs, int64_t* job_uid, int64_t* uid_base,
                                  unsigned long long* job_words, unsigned long long* job_kept,
                                  int64_t* entry_prefix, cudaStream_t st);
-extern template cudaError_t batch_grid<float, 0>(int64_t, int, int, int, int64_t, int, int*, int*, size_t*);
-extern template cudaError_t batch_grid<float, 1>(int64_t, int, int, int, int64_t, int, int*, int*, size_t*);
-extern template cudaError_t batch_grid<bf16_t, 0>(int64_t, int, int, int, int64_t, int, int*, int*, size_t*);
-extern template cudaError_t batch_grid<bf16_t, 1>(int64_t, int, int, int, int64_t, int, int*, int*, size_t*);
-extern template cudaError_t batch_launch<float, 0>(const BatchTrainArgs&, int, int, size_t, cudaStream_t);
-extern template cudaError_t batch_launch<float, 1>(const BatchTrainArgs&, int, int, size_t, cudaStream_t);
-extern template cudaError_t batch_launch<bf16_t, 0>(const BatchTrainArgs&, int, int, size_t, cudaStream_t);
-extern template cudaError_t batch_launch<bf16_t, 1>(const BatchTrainArgs&, int, int, size_t, cudaStream_t);
+#define FW2V_BATCH_EXTERN(T, F)                                                                     \
+  extern template cudaError_t batch_grid<T, F>(int64_t, int, int, int, int64_t, int, int*, int*, size_t*); \
+  extern template cudaError_t batch_launch<T, F>(const BatchTrainArgs&, int, int, size_t, cudaStream_t);
+FW2V_BATCH_EXTERN(float, 0)
+FW2V_BATCH_EXTERN(float, 1)
+FW2V_BATCH_EXTERN(float, 2)
+FW2V_BATCH_EXTERN(bf16_t, 0)
+FW2V_BATCH_EXTERN(bf16_t, 1)
+FW2V_BATCH_EXTERN(bf16_t, 2)
+#undef FW2V_BATCH_EXTERN
 }  // namespace fw2v
 
 using namespace fw2v;
@@ -70,7 +72,7 @@ struct BatchJob {
   std::vector<int64_t> sbase;  // threads + 1: readable-token prefix of its streams
   int64_t gfirst = 0;          // global number of its stream 0
   int lane_vec = 4, lane_nv = 1, stages = 6;
-  int family() const { return lane_nv >= 2 ? 1 : 0; }
+  int family() const { return batch_family(lane_nv, stages); }
 };
 
 struct RoundPlan {
@@ -167,7 +169,7 @@ struct fw2v_batch {
   int64_t buf_kept_cap = 0, buf_stream_cap = 0;
   void* orig_scratch = nullptr;
   int64_t scratch_elems = 0, scratch_warps = 0, scratch_bytes = 0;
-  int warps_per_block[2] = {4, 4}, blocks_per_sm[2] = {0, 0};  // per kernel family
+  int warps_per_block[kBatchFamilies] = {4, 4, 4}, blocks_per_sm[kBatchFamilies] = {0, 0, 0};  // per family
   int epochs_run = 0;  // batch epochs trained so far: job j has trained min(epochs_run, its epochs)
 };
 
@@ -238,7 +240,7 @@ void free_plan(fw2v_batch* b) {
 }
 
 int64_t shape_smem_floats(const BatchJob& j) {
-  return (int64_t)(2 * j.cfg.window + 1 + 3 + j.stages) * j.pitch;
+  return (int64_t)WarpRows<1>::rows(2 * j.cfg.window + 1) * j.pitch + 2 * (int64_t)(j.stages - 1) * j.pitch;
 }
 int64_t shape_scratch_elems(const BatchJob& j) { return (int64_t)(2 * j.cfg.window + 1) * j.pitch; }
 
@@ -315,7 +317,7 @@ fw2v_status plan(fw2v_batch* b) {
     int64_t gstream, tokens;
   };
   const int64_t cap = b->cfg.round_tokens > 0 ? b->cfg.round_tokens : (int64_t)1 << 27;
-  for (int fam = 0; fam < 2; fam++) {
+  for (int fam = 0; fam < kBatchFamilies; fam++) {
   std::vector<Item> order;
   int max_t = 0;
   for (const BatchJob& j : b->jobs)
@@ -424,17 +426,17 @@ fw2v_status grid_for(fw2v_batch* b, const std::vector<int>& active, int fam, int
     if (b->jobs[j].family() == fam) g->smem_floats = std::max(g->smem_floats, shape_smem_floats(b->jobs[j]));
   if (g->smem_floats == 0) return FW2V_OK;
   const int det = b->cfg.deterministic;
-  cudaError_t e;
-  if (b->elem == 2)
-    e = fam ? batch_grid<bf16_t, 1>(g->smem_floats, wpb, cap, b->num_sms, b->scratch_warps, det, &g->blocks,
-                                    &g->threads, &g->smem)
-            : batch_grid<bf16_t, 0>(g->smem_floats, wpb, cap, b->num_sms, b->scratch_warps, det, &g->blocks,
-                                    &g->threads, &g->smem);
-  else
-    e = fam ? batch_grid<float, 1>(g->smem_floats, wpb, cap, b->num_sms, b->scratch_warps, det, &g->blocks,
-                                   &g->threads, &g->smem)
-            : batch_grid<float, 0>(g->smem_floats, wpb, cap, b->num_sms, b->scratch_warps, det, &g->blocks,
-                                   &g->threads, &g->smem);
+  cudaError_t e = cudaErrorInvalidValue;
+#define FW2V_GRID(T, F)                                                                                  \
+  if (fam == F)                                                                                         \
+    e = batch_grid<T, F>(g->smem_floats, wpb, cap, b->num_sms, b->scratch_warps, det, &g->blocks, &g->threads, \
+                         &g->smem);
+  if (b->elem == 2) {
+    FW2V_GRID(bf16_t, 0) FW2V_GRID(bf16_t, 1) FW2V_GRID(bf16_t, 2)
+  } else {
+    FW2V_GRID(float, 0) FW2V_GRID(float, 1) FW2V_GRID(float, 2)
+  }
+#undef FW2V_GRID
   if (e != cudaSuccess)
     return bfail(b, FW2V_ERR_ARGUMENT, "batch grid (%d warps per block, %lld floats per warp): %s", wpb,
                  (long long)g->smem_floats, cudaGetErrorString(e));
@@ -463,11 +465,14 @@ BatchTrainArgs train_args(const fw2v_batch* b, const RoundBuf& rb, const BatchRo
 
 cudaError_t launch_train_round(const fw2v_batch* b, int fam, const BatchTrainArgs& a, const Grid& g,
                                cudaStream_t st) {
-  if (b->elem == 2)
-    return fam ? batch_launch<bf16_t, 1>(a, g.blocks, g.threads, g.smem, st)
-               : batch_launch<bf16_t, 0>(a, g.blocks, g.threads, g.smem, st);
-  return fam ? batch_launch<float, 1>(a, g.blocks, g.threads, g.smem, st)
-             : batch_launch<float, 0>(a, g.blocks, g.threads, g.smem, st);
+  if (b->elem == 2) {
+    if (fam == 0) return batch_launch<bf16_t, 0>(a, g.blocks, g.threads, g.smem, st);
+    if (fam == 1) return batch_launch<bf16_t, 1>(a, g.blocks, g.threads, g.smem, st);
+    return batch_launch<bf16_t, 2>(a, g.blocks, g.threads, g.smem, st);
+  }
+  if (fam == 0) return batch_launch<float, 0>(a, g.blocks, g.threads, g.smem, st);
+  if (fam == 1) return batch_launch<float, 1>(a, g.blocks, g.threads, g.smem, st);
+  return batch_launch<float, 2>(a, g.blocks, g.threads, g.smem, st);
 }
 
 // Sample one round into buffer set rb on the sampler stream.
@@ -741,7 +746,7 @@ fw2v_status fw2v_batch_set_shape(fw2v_batch* b, int32_t job, int32_t lane_vec, i
   if (!valid_shape(j.cfg.layer_size, lane_vec, lane_nv, stages))
     return bfail(b, FW2V_ERR_ARGUMENT, "shape (%d x %d, %d stages) cannot train d = %d", lane_vec, lane_nv, stages,
                  j.cfg.layer_size);
-  if ((lane_nv >= 2) != (j.family() == 1)) b->planned = false;  // the job moves to the other kernel family
+  if (batch_family(lane_nv, stages) != j.family()) b->planned = false;  // the job moves to another family
   j.lane_vec = lane_vec;
   j.lane_nv = lane_nv;
   j.stages = stages;
@@ -758,15 +763,17 @@ fw2v_status fw2v_batch_get_shape(fw2v_batch* b, int32_t job, int32_t* lane_vec, 
 }
 
 fw2v_status fw2v_batch_set_launch(fw2v_batch* b, int32_t family, int32_t warps_per_block, int32_t blocks_per_sm) {
-  if (!b || family < 0 || family > 1 || warps_per_block < 1 || warps_per_block > kBatchMaxWarps || blocks_per_sm < 0)
-    return bfail(b, FW2V_ERR_ARGUMENT, "family 0 or 1, warps per block 1..8, blocks per SM >= 0");
+  const int max_w = family == 0 ? BatchFamily<0>::kMaxWarps : BatchFamily<1>::kMaxWarps;
+  if (!b || family < 0 || family >= kBatchFamilies || warps_per_block < 1 || warps_per_block > max_w ||
+      blocks_per_sm < 0)
+    return bfail(b, FW2V_ERR_ARGUMENT, "family 0..2, warps per block 1..8 (1..4 for wide rows), blocks per SM >= 0");
   b->warps_per_block[family] = warps_per_block;
   b->blocks_per_sm[family] = blocks_per_sm;
   return FW2V_OK;
 }
 
 fw2v_status fw2v_batch_get_launch(fw2v_batch* b, int32_t family, int32_t* warps_per_block, int32_t* blocks_per_sm) {
-  if (!b || family < 0 || family > 1 || !warps_per_block || !blocks_per_sm) return FW2V_ERR_ARGUMENT;
+  if (!b || family < 0 || family >= kBatchFamilies || !warps_per_block || !blocks_per_sm) return FW2V_ERR_ARGUMENT;
   *warps_per_block = b->warps_per_block[family];
   *blocks_per_sm = b->blocks_per_sm[family];
   return FW2V_OK;
@@ -781,8 +788,8 @@ fw2v_status fw2v_batch_train_epochs(fw2v_batch* b, int32_t n_epochs, fw2v_batch_
   if (s != FW2V_OK) return s;
   std::vector<int> all(b->jobs.size());
   for (size_t i = 0; i < all.size(); i++) all[i] = (int)i;
-  Grid g[2];
-  for (int fam = 0; fam < 2; fam++) {
+  Grid g[kBatchFamilies];
+  for (int fam = 0; fam < kBatchFamilies; fam++) {
     s = grid_for(b, all, fam, b->warps_per_block[fam], b->blocks_per_sm[fam], &g[fam]);
     if (s != FW2V_OK) return s;
   }
@@ -1016,7 +1023,6 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
     const BatchJob& j0 = b->jobs[members[c][0]];
     const int def_vec = j0.pitch <= 64 ? 2 : 4, def_nv = j0.pitch <= 128 ? 1 : (j0.pitch <= 256 ? 2 : 3);
     const int def_st = default_stages(b->negative, def_nv);
-    const int fam = def_nv >= 2 ? 1 : 0;
     double best = -1, def_wps = 0;
     int best_vec = def_vec, best_nv = def_nv, best_st = def_st;
     for (int vec : {2, 4}) {
@@ -1028,6 +1034,7 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
           b->jobs[j].stages = st;
         }
         float ms = 0;
+        const int fam = batch_family(def_nv, st);
         result = time_round(b, r, members[c], fam, b->warps_per_block[fam], b->blocks_per_sm[fam], 2, &ms);
         if (result != FW2V_OK) break;
         const double wps = kept / (ms / 1e3);
@@ -1054,13 +1061,13 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
     bfree(r.dev);
   }
   // grid of each kernel family: warps per block over all its jobs together
-  for (int fam = 0; fam < 2 && result == FW2V_OK; fam++) {
+  for (int fam = 0; fam < kBatchFamilies && result == FW2V_OK; fam++) {
     std::vector<int> act;
     for (size_t i = 0; i < J; i++)
       if (b->jobs[i].family() == fam) act.push_back((int)i);
     if (act.empty()) continue;
     int n_cls = 0;
-    for (size_t c = 0; c < keys.size(); c++) n_cls += (keys[c].first >= 2) == (fam == 1);
+    for (size_t c = 0; c < keys.size(); c++) n_cls += b->jobs[members[c][0]].family() == fam;
     RoundPlan r;
     result = tuning_round(b, act, sample_tokens * (int64_t)std::max(n_cls, 1), &r);
     if (result == FW2V_OK) result = sample_into_buf0(r);
@@ -1068,6 +1075,7 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
     int best_w = b->warps_per_block[fam];
     for (int w : {2, 4, 8}) {
       if (result != FW2V_OK) break;
+      if (fam != 0 && w > BatchFamily<1>::kMaxWarps) continue;
       Grid g;
       if (grid_for(b, act, fam, w, 0, &g) != FW2V_OK) continue;  // does not fit: skip
       float ms = 0;
@@ -1081,7 +1089,7 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
     b->blocks_per_sm[fam] = 0;
     bfree(r.dev);
   }
-  for (int fam = 0; fam < 2; fam++) {
+  for (int fam = 0; fam < kBatchFamilies; fam++) {
     rep.warps_per_block[fam] = b->warps_per_block[fam];
     rep.blocks_per_sm[fam] = b->blocks_per_sm[fam];
   }

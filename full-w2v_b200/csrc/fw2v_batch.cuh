@@ -41,21 +41,35 @@ struct BatchTrainArgs {
 // per centre sweeps them in ceil((1 + K) / stages) groups).
 constexpr int kBatchStages[] = {2, 3, 4, 6};
 
-// Kernel families: rows of one vector per lane (d <= 128: 2-float lanes for
-// d <= 64, 4-float for d <= 128) within 128 registers and up to 16 warps per
-// SM; and wide rows of 2 or 3 four-float vectors per lane (d <= 384) with up
-// to 255 registers.
+// Kernel families, each compiled for its own register budget (the largest of
+// its bodies sets it for all):
+//   0  rows of one vector per lane (d <= 128: 2-float lanes for d <= 64,
+//      4-float for d <= 128), up to 8 warps per block, 128 registers
+//   1  wide rows, light pipelines: 2 four-float vectors per lane with 2 or 3
+//      stages, 3 vectors with 2 stages; 4 warps per block, 3 blocks per SM
+//   2  wide rows, deep pipelines: 2 vectors with 4 or 6 stages, 3 vectors
+//      with 3 or 4; 4 warps per block, 255 registers
 constexpr int kBatchMaxWarps = 8;
+constexpr int kBatchFamilies = 3;
 template <int FAMILY>
 struct BatchFamily;
 template <>
 struct BatchFamily<0> {
-  static constexpr int kMinBlocks = 2;
+  static constexpr int kMaxWarps = 8, kMinBlocks = 2;
 };
 template <>
 struct BatchFamily<1> {
-  static constexpr int kMinBlocks = 1;
+  static constexpr int kMaxWarps = 4, kMinBlocks = 3;
 };
+template <>
+struct BatchFamily<2> {
+  static constexpr int kMaxWarps = 4, kMinBlocks = 2;
+};
+
+// The family of a (lane vector width, vectors per lane, stages) shape.
+__host__ __device__ constexpr int batch_family(int nv, int stages) {
+  return nv == 1 ? 0 : ((nv == 2 && stages <= 3) || (nv == 3 && stages <= 2)) ? 1 : 2;
+}
 
 // Rows of three vectors per lane stop at 4 stages: their 6-stage body does not
 // fit the register file.
@@ -78,14 +92,23 @@ __device__ __forceinline__ void batch_dispatch(const TrainParams& p, const Sente
   if constexpr (FAMILY == 0) {
     if (p.lane_vec == 2) batch_stages<T, 2, 1>(p, sn, ring, orig, table, lane);
     else batch_stages<T, 4, 1>(p, sn, ring, orig, table, lane);
+  } else if constexpr (FAMILY == 1) {
+    if (p.lane_nv == 3) train_sentence<T, 4, 3, 2, 0>(p, sn, ring, orig, table, lane);
+    else if (p.stages == 2) train_sentence<T, 4, 2, 2, 0>(p, sn, ring, orig, table, lane);
+    else train_sentence<T, 4, 2, 3, 0>(p, sn, ring, orig, table, lane);
   } else {
-    if (p.lane_nv == 2) batch_stages<T, 4, 2>(p, sn, ring, orig, table, lane);
-    else batch_stages<T, 4, 3>(p, sn, ring, orig, table, lane);
+    if (p.lane_nv == 3) {
+      if (p.stages == 3) train_sentence<T, 4, 3, 3, 0>(p, sn, ring, orig, table, lane);
+      else train_sentence<T, 4, 3, 4, 0>(p, sn, ring, orig, table, lane);
+    } else {
+      if (p.stages == 4) train_sentence<T, 4, 2, 4, 0>(p, sn, ring, orig, table, lane);
+      else train_sentence<T, 4, 2, 6, 0>(p, sn, ring, orig, table, lane);
+    }
   }
 }
 
 template <typename T, int FAMILY>
-__global__ void __launch_bounds__(kBatchMaxWarps * 32, BatchFamily<FAMILY>::kMinBlocks)
+__global__ void __launch_bounds__(BatchFamily<FAMILY>::kMaxWarps * 32, BatchFamily<FAMILY>::kMinBlocks)
     sgns_batch_kernel(BatchTrainArgs a) {
   extern __shared__ __align__(16) float smem[];
   __shared__ __align__(8) TrainParams tp[kBatchMaxWarps];
@@ -148,7 +171,7 @@ cudaError_t batch_grid(int64_t smem_floats, int warps, int per_sm_cap, int num_s
                        int deterministic, int* blocks, int* threads, size_t* smem) {
   auto kern = sgns_batch_kernel<T, FAMILY>;
   if (deterministic) warps = 1;
-  if (warps < 1 || warps > kBatchMaxWarps) return cudaErrorInvalidValue;
+  if (warps < 1 || warps > BatchFamily<FAMILY>::kMaxWarps) return cudaErrorInvalidValue;
   *smem = (size_t)warps * (size_t)smem_floats * sizeof(float);
   *threads = warps * 32;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);

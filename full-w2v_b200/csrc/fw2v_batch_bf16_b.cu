@@ -1,4 +1,4 @@
-// Instantiation of the batched training kernel: bfloat16 tables, wide rows (128 < d <= 384).
+// Instantiation of the batched training kernel: bfloat16 tables, wide rows, light pipelines.
 #include "fw2v_batch.cuh"
 
 namespace fw2v {

@@ -46,14 +46,15 @@ LaunchShape choose_shape(int d, int negative) {
   }
   const int want = negative + 1;
   s.r = want <= 1 ? 1 : want <= 2 ? 2 : want <= 4 ? 4 : want <= 6 ? 6 : 8;
+  if (s.nv == 3 && s.r > 4) s.r = 4;  // three vectors per lane: more stages spill registers
   if (s.nv >= 4) s.r = 1;
   return s;
 }
 
-// Shared memory of one block: per warp, the ring of 2W+1 rows, a sink row, R
-// target originals and two staging rows (WarpRows).
+// Shared memory of one block: per warp, the ring of 2W+1 rows, a sink row, two
+// sets of R target rows and two staging rows (WarpRows).
 size_t train_smem_bytes(int window, int64_t pitch, int warps, int r) {
-  return (size_t)warps * (2 * window + 1 + 3 + r) * pitch * sizeof(float);
+  return (size_t)warps * (2 * window + 1 + 3 + 2 * r) * pitch * sizeof(float);
 }
 
 // Warps the scratch of a handle must cover: every warp the persistent grid can

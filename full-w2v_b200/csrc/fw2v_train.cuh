@@ -563,7 +563,7 @@ __device__ __forceinline__ void lds_staged(Row<VEC, NV>& r, uint32_t row, const 
 // Shared-memory rows of one warp, each `P` floats.
 template <int R>
 struct WarpRows {
-  static constexpr int kExtra = 1 + R + 2;  // sink, R target originals, 2 staging rows
+  static constexpr int kExtra = 1 + 2 * R + 2;  // sink, 2 x R target rows, 2 staging rows
   __host__ __device__ static constexpr int rows(int D) { return D + kExtra; }
 };
 
@@ -619,9 +619,21 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   const uint32_t ring_b = smem_addr(ring);
   const uint32_t row_bytes = (uint32_t)P * 4u;
   const uint32_t sink_b = ring_b + (uint32_t)D * row_bytes;
+  // Target rows: two sets of R rows.  With all 1 + K targets of a centre in
+  // one group, centre w's rows were copied (cp.async, table element type)
+  // into set w % 2 while centre w-1 trained, and are kept there as the
+  // originals for the write-back; otherwise set 0 holds the FP32 originals of
+  // the current group.
   const uint32_t o0_b = sink_b + row_bytes;
-  const uint32_t in_b = o0_b + (uint32_t)R * row_bytes;
+  const uint32_t o1_b = o0_b + (uint32_t)R * row_bytes;
+  const uint32_t in_b = o1_b + (uint32_t)R * row_bytes;
   const uint32_t out_b = in_b + row_bytes;
+  auto prefetch_targets = [&](uint32_t set, int my_target) {
+    for (int k = 0; k <= K; k++) {
+      const int tk = __shfl_sync(kFull, my_target, k);
+      cp_row(set + (uint32_t)k * row_bytes, syn1neg + (int64_t)tk * P, lm, d);
+    }
+  };
 
   // v[r] holds the context row whose index j in the centre's list has
   // j % R == r: stage k works on context t-k at step t, i.e. on register slot
@@ -635,13 +647,23 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   }
 
   int t_next = one_group ? target_id(ids, negs, K, 0, 0, K + 1, lane) : 0;
+  if (one_group) {
+    prefetch_targets(o0_b, t_next);
+    cp_async_commit();
+    cp_async_wait();
+  }
+  int t_prev = -1;  // lane k: target k of the previous centre if it wrote it back
   for (int w = 0; w < L; w++) {
     // Ids and rows needed later in this centre, loaded ahead of use.
     const int q_out = w - W, q_in = w + W + 1;
     const int id_out = q_out >= 0 ? __ldg(ids + q_out) : -1;
     const int id_in = q_in < L ? __ldg(ids + q_in) : -1;
     const int t_here = t_next;
-    if (one_group && w + 1 < L) t_next = target_id(ids, negs, K, w + 1, 0, K + 1, lane);
+    const uint32_t cur_b = (w & 1) ? o1_b : o0_b;
+    if (one_group && w + 1 < L) {
+      t_next = target_id(ids, negs, K, w + 1, 0, K + 1, lane);
+      prefetch_targets((w & 1) ? o0_b : o1_b, t_next);
+    }
     // The entering row can be fetched now unless the leaving position holds
     // the same word (its write-back must land first).  Both staging copies run
     // in the background while the centre trains.
@@ -676,8 +698,22 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
           for (int k = 0; k < R; k++) {
             const int tk = __shfl_sync(kFull, my_t, k);
             if (k < nt) {
-              row_load_global(o[k], syn1neg + (int64_t)tk * P, lane, d);
-              sts_row(o[k], o0_b + (uint32_t)k * row_bytes, lm);
+              if (one_group) {
+                // The copy was taken before the previous centre's write-back:
+                // a target it also wrote is fetched again (after this lane's
+                // own reduction, in program order).
+                bool stale = false;
+                for (int j = 0; j <= K; j++) stale |= __shfl_sync(kFull, t_prev, j) == tk;
+                if (stale) {
+                  cp_row(cur_b + (uint32_t)k * row_bytes, syn1neg + (int64_t)tk * P, lm, d);
+                  cp_async_commit();
+                  cp_async_wait();
+                }
+                lds_staged<T>(o[k], cur_b + (uint32_t)k * row_bytes, lm);
+              } else {
+                row_load_global(o[k], syn1neg + (int64_t)tk * P, lane, d);
+                sts_row(o[k], o0_b + (uint32_t)k * row_bytes, lm);
+              }
             } else {
               row_zero(o[k]);
             }
@@ -724,7 +760,8 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
             const int tk = __shfl_sync(kFull, my_t, k);
             if (k < nt) {
               Row<VEC, NV> o0;
-              lds_row(o0, o0_b + (uint32_t)k * row_bytes, lm);
+              if (one_group) lds_staged<T>(o0, cur_b + (uint32_t)k * row_bytes, lm);
+              else lds_row(o0, o0_b + (uint32_t)k * row_bytes, lm);
               row_add_delta(syn1neg + (int64_t)tk * P, o[k], o0, lane, d,
                             sr_event_key(skey, (uint64_t)w * (K + 1) + (k0 + k)),
                             (uint64_t)tk);
@@ -755,6 +792,8 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
         }
       }
     }
+
+    t_prev = nctx > 0 ? t_here : -1;
 
     // Slide the window: position w-W leaves, position w+W+1 takes its slot.
     cp_async_wait();

@@ -62,8 +62,8 @@ class TuneReport(C.Structure):
     _fields_ = [("n_classes", C.c_int32), ("class_d", C.c_int32 * 16), ("class_window", C.c_int32 * 16),
                 ("class_lane_vec", C.c_int32 * 16), ("class_lane_nv", C.c_int32 * 16),
                 ("class_stages", C.c_int32 * 16), ("tuned_wps", C.c_double * 16),
-                ("default_wps", C.c_double * 16), ("warps_per_block", C.c_int32 * 2),
-                ("blocks_per_sm", C.c_int32 * 2)]
+                ("default_wps", C.c_double * 16), ("warps_per_block", C.c_int32 * 3),
+                ("blocks_per_sm", C.c_int32 * 3)]
 
 
 # Every entry point declared in include/fw2v.h (tests check the library exports them all).
@@ -417,7 +417,7 @@ class Batch:
         import json
 
         keys = [self._class_key(c) for c, _ in self.jobs]
-        launch_keys = [f"launch{f}:{self._device_key()}" for f in (0, 1)]
+        launch_keys = [f"launch{f}:{self._device_key()}" for f in (0, 1, 2)]
         store = {}
         if cache and os.path.exists(cache):
             with open(cache) as f:

@@ -249,8 +249,9 @@ const char* fw2v_version(void);
  *
  * Jobs: layer_size <= 384, sigmoid FW2V_SIGMOID_TABLE, the same `negative` in
  * every job of a batch; the batch's precision and deterministic flags replace
- * the jobs' own.  Jobs with one vector per lane (d <= 128) and wide jobs (2 or
- * 3 vectors per lane) run in separate rounds on two kernel families. */
+ * the jobs' own.  Jobs run in rounds of one kernel family each: one vector per
+ * lane (d <= 128), and wide rows (2 or 3 vectors per lane) with light or deep
+ * pipelines, each family compiled for its own register budget. */
 typedef struct fw2v_batch fw2v_batch;
 
 typedef struct fw2v_batch_config {
@@ -290,9 +291,10 @@ fw2v_status fw2v_batch_set_shape(fw2v_batch* b, int32_t job, int32_t lane_vec, i
 fw2v_status fw2v_batch_get_shape(fw2v_batch* b, int32_t job, int32_t* lane_vec, int32_t* lane_nv,
                                  int32_t* stages);
 
-/* The training grid of a kernel family (0: one vector per lane, 1: wide
- * rows): warps per block (sentences trained side by side in one block, 1..8)
- * and a cap on blocks per SM (0: as many as fit). */
+/* The training grid of a kernel family (0: one vector per lane; 1: wide rows
+ * with 2 or 3 stages (2 vectors per lane) or 2 stages (3 vectors); 2: other
+ * wide rows): warps per block (sentences trained side by side in one block,
+ * 1..8, 1..4 for wide rows) and a cap on blocks per SM (0: as many as fit). */
 fw2v_status fw2v_batch_set_launch(fw2v_batch* b, int32_t family, int32_t warps_per_block, int32_t blocks_per_sm);
 fw2v_status fw2v_batch_get_launch(fw2v_batch* b, int32_t family, int32_t* warps_per_block,
                                   int32_t* blocks_per_sm);
@@ -307,7 +309,7 @@ typedef struct fw2v_batch_tune_report {
   int32_t n_classes;
   int32_t class_d[16], class_window[16], class_lane_vec[16], class_lane_nv[16], class_stages[16];
   double tuned_wps[16], default_wps[16];
-  int32_t warps_per_block[2], blocks_per_sm[2];  /* per kernel family */
+  int32_t warps_per_block[3], blocks_per_sm[3];  /* per kernel family */
 } fw2v_batch_tune_report;
 fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2v_batch_tune_report* report);
 

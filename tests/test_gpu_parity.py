@@ -389,17 +389,22 @@ def test_bf16_per_step_error_within_stated_bound_of_fp64():
         assert 0 < worst <= 1.0, worst
 
 
-def test_bf16_hogwild_learns_like_fp32():
+def test_bf16_learns_like_fp32():
+    """Two epochs one sentence at a time: bfloat16 tables end with the FP32
+    loss to 0.5% (the oracle's restatement gives 0.004% on this corpus); with
+    Hogwild both learn and stay finite."""
     g = load("zipf_t1")
     c = dict(g["cfg"])
     corpus = corpus_of(g)
     lens, alphas, ids, negs = _flatten_epoch(_oracle_epoch(corpus, dict(c, iter=1)), 0)
     losses = {}
     for prec in (fw2v.FP32, fw2v.BF16):
-        with trainer_for(corpus, c, layer_size=64, precision=prec) as t:
-            before, _ = t.heldout_loss(lens, ids, negs)
-            assert t.train() == int(g["overall_words"])
-            after, _ = t.heldout_loss(lens, ids, negs)
-            assert np.isfinite(t.syn0()).all() and after < before
-            losses[prec] = after
-    assert abs(losses[fw2v.BF16] - losses[fw2v.FP32]) <= 0.02 * losses[fw2v.FP32]
+        for det in (1, 0):
+            with trainer_for(corpus, c, layer_size=64, precision=prec, deterministic=det) as t:
+                before, _ = t.heldout_loss(lens, ids, negs)
+                assert t.train() == int(g["overall_words"])
+                after, _ = t.heldout_loss(lens, ids, negs)
+                assert np.isfinite(t.syn0()).all() and after < before
+                if det:
+                    losses[prec] = after
+    assert abs(losses[fw2v.BF16] - losses[fw2v.FP32]) <= 0.005 * losses[fw2v.FP32]
