@@ -41,7 +41,10 @@ struct Options {
   bool do_export = true, recount = false, cache_eos = false, pre_shuffle = false, epoch_shuffle = false;
   int binary = 0, debug = 2, min_count = 5, layer_size = 100, epochs = 5, window = 5, negative = 5;
   int threads = -1, msl = 1000, sigmoid = FW2V_SIGMOID_TABLE, deterministic = 0, device = 0;
+  int precision = FW2V_FP32, tune = 1;
+  unsigned long long seed = 0;
   float alpha = 0.025f, sample = 1e-3f;
+  std::string jobs;  // manifest: one job's arguments per line, trained together
 };
 
 // ---------------------------------------------------------------------------
@@ -383,6 +386,12 @@ void usage(const char* prog) {
   printf("\t-negative(s) <int>\tNegative examples; default 5 (0..31)\n");
   printf("\t-sigmoid table|exact\tSigmoid: the reference's 1000-entry table (default) or exact\n");
   printf("\t-deterministic 0|1\tTrain sentences one at a time in stream order\n");
+  printf("\t-precision fp32|bf16\tEmbedding tables in FP32 (default) or bfloat16 with stochastic rounding\n");
+  printf("\t-seed <int>\t\t0 (default): the reference's seeds; otherwise offsets every LCG start\n");
+  printf("** MANY JOBS **\n");
+  printf("\t-jobs <file>\t\tTrain the jobs listed in <file> (one job's options per line, '#' comments)\n");
+  printf("\t\t\t\ttogether on one GPU; -precision, -device, -deterministic apply to all\n");
+  printf("\t-tune 0|1\t\tWith -jobs, pick kernel shapes by measurement first (default 1)\n");
   printf("** PARALLEL UTILIZATION **\n");
   printf("\t-thread(s) <int>\tSampling streams (the reference's CPU threads); default: one per 256 sentences\n");
   printf("\t-max-sentence-length, -msl <int>\tMaximum sentence length; default 1000\n");
@@ -432,7 +441,28 @@ bool parse(int argc, char** argv, Options& o) {
   if (const char* v = val("-sigmoid")) o.sigmoid = !strcmp(v, "exact") ? FW2V_SIGMOID_EXACT : FW2V_SIGMOID_TABLE;
   if (const char* v = val("-deterministic")) o.deterministic = atoi(v);
   if (const char* v = val("-device")) o.device = atoi(v);
+  if (const char* v = val("-precision")) o.precision = !strcmp(v, "bf16") ? FW2V_BF16 : FW2V_FP32;
+  if (const char* v = val("-seed")) o.seed = strtoull(v, nullptr, 10);
+  if (const char* v = val("-jobs")) o.jobs = v;
+  if (const char* v = val("-tune")) o.tune = atoi(v);
   return true;
+}
+
+// The options of one manifest line, on top of defaults.
+bool parse_line(const std::string& line, Options& o) {
+  std::vector<std::string> toks;
+  size_t i = 0;
+  while (i < line.size()) {
+    while (i < line.size() && isspace((unsigned char)line[i])) i++;
+    size_t j = i;
+    while (j < line.size() && !isspace((unsigned char)line[j])) j++;
+    if (j > i) toks.push_back(line.substr(i, j - i));
+    i = j;
+  }
+  if (toks.empty() || toks[0][0] == '#') return false;
+  std::vector<char*> argv{(char*)"full-w2v"};
+  for (std::string& t : toks) argv.push_back(&t[0]);
+  return parse((int)argv.size(), argv.data(), o);
 }
 
 int fail_status(const char* what, fw2v_status s, fw2v_handle* h) {
@@ -442,22 +472,10 @@ int fail_status(const char* what, fw2v_status s, fw2v_handle* h) {
 
 }  // namespace
 
-int main(int argc, char** argv) {
-  Options o;
-  if (!parse(argc, argv, o)) return 0;
-  if (o.debug > 0) {
-    fprintf(stderr, "** FILES & I/O **\n");
-    if (!o.do_export && !o.output.empty()) fprintf(stderr, "!!\tProcess will train but will not export a model!\n");
-    else if (!o.output.empty()) fprintf(stderr, "Trained model will export to file: %s\n", o.output.c_str());
-    else fprintf(stderr, "!!\tPreprocessing only -- no training.\n");
-    fprintf(stderr, "layer size: %d, epochs: %d, alpha: %.5f, window: %d, sample: %f, negative: %d\n",
-            o.layer_size, o.epochs, o.alpha, o.window, o.sample, o.negative);
-  }
-
-  // SetupNetwork (FULL-W2V-driver.cu:356-425)
-  Vocab vocab;
-  Corpus corpus;
-  uint64_t train_words = 0;
+// SetupNetwork (FULL-W2V-driver.cu:356-425): vocabulary, corpus stream and
+// chunks, the caches and the stream count.  Returns 0 to go on training, -1
+// when there is nothing to train (preprocessing only), or a process exit code.
+int prepare(Options& o, Vocab& vocab, Corpus& corpus, uint64_t& train_words) {
   if (!o.train.empty()) {
     Mapped f;
     if (!f.open(o.train)) {
@@ -509,14 +527,16 @@ int main(int argc, char** argv) {
   if (o.debug > 1)
     printf("%lld sentences spread across %d sampling streams == %lld sentences/stream\n", (long long)n_chunks,
            o.threads, (long long)(n_chunks / std::max(o.threads, 1)));
-  if (o.output.empty()) return 0;
+  if (o.output.empty()) return -1;
   if (n_chunks == 0) {
     printf("ERROR: the corpus holds no in-vocabulary words\n");
     return 1;
   }
-  if (o.pre_shuffle) shuffle_chunks(corpus.chunk_off);
 
-  // InitNet + Train_SGNS through libfw2v
+  return 0;
+}
+
+fw2v_config job_config(const Options& o) {
   fw2v_config cfg;
   fw2v_config_default(&cfg);
   cfg.layer_size = o.layer_size;
@@ -530,6 +550,120 @@ int main(int argc, char** argv) {
   cfg.sigmoid = o.sigmoid;
   cfg.deterministic = o.deterministic;
   cfg.device = o.device;
+  cfg.precision = o.precision;
+  cfg.seed = o.seed;
+  return cfg;
+}
+
+int batch_fail(const char* what, fw2v_status st, fw2v_batch* b) {
+  fprintf(stderr, "ERROR: %s: %s: %s\n", what, fw2v_status_string(st), b ? fw2v_batch_last_error(b) : "");
+  fw2v_batch_destroy(b);
+  return 1;
+}
+
+// -jobs: every manifest line is one job's command line; all jobs train
+// together in one libfw2v batch and each exports its own vectors.
+int run_jobs(const Options& g) {
+  std::FILE* f = std::fopen(g.jobs.c_str(), "r");
+  if (!f) {
+    printf("ERROR: job manifest \"%s\" not found!\n", g.jobs.c_str());
+    return 1;
+  }
+  std::vector<Options> opts;
+  char buf[1 << 14];
+  while (std::fgets(buf, sizeof(buf), f)) {
+    Options o;
+    o.debug = 0;
+    if (!parse_line(buf, o)) continue;
+    o.precision = g.precision;  // batch-wide settings
+    o.device = g.device;
+    o.deterministic = g.deterministic;
+    opts.push_back(o);
+  }
+  std::fclose(f);
+  if (opts.empty()) {
+    printf("ERROR: the job manifest lists no jobs\n");
+    return 1;
+  }
+  fw2v_batch_config bc;
+  fw2v_batch_config_default(&bc);
+  bc.precision = g.precision;
+  bc.device = g.device;
+  bc.deterministic = g.deterministic;
+  fw2v_batch* b = nullptr;
+  fw2v_status st = fw2v_batch_create(&bc, &b);
+  if (st != FW2V_OK) return fail_status("batch_create", st, nullptr);
+  std::vector<Vocab> vocabs(opts.size());
+  for (size_t j = 0; j < opts.size(); j++) {
+    Corpus corpus;
+    uint64_t train_words = 0;
+    if (const int r = prepare(opts[j], vocabs[j], corpus, train_words)) {
+      fw2v_batch_destroy(b);
+      if (r < 0) printf("ERROR: job %zu has no -output\n", j + 1);
+      return 1;
+    }
+    if (opts[j].pre_shuffle) shuffle_chunks(corpus.chunk_off);
+    std::vector<uint32_t> counts(vocabs[j].counts.size());
+    for (size_t i = 0; i < counts.size(); i++) counts[i] = (uint32_t)vocabs[j].counts[i];
+    const fw2v_config cfg = job_config(opts[j]);
+    int32_t id = 0;
+    st = fw2v_batch_add_job(b, &cfg, counts.data(), (int64_t)counts.size(), train_words, corpus.stream.data(),
+                            (int64_t)corpus.stream.size(), corpus.chunk_off.data(),
+                            (int64_t)corpus.chunk_off.size(), &id);
+    if (st != FW2V_OK) return batch_fail("add job", st, b);
+  }
+  if (g.tune && !g.deterministic) {
+    fw2v_batch_tune_report rep;
+    if ((st = fw2v_batch_tune(b, 0, &rep)) != FW2V_OK) return batch_fail("tune", st, b);
+  }
+  const double t0 = now_s();
+  fw2v_batch_stats bs;
+  if ((st = fw2v_batch_train(b, &bs)) != FW2V_OK) return batch_fail("train", st, b);
+  const double t1 = now_s();
+  for (size_t j = 0; j < opts.size(); j++) {
+    uint64_t wr = 0, wk = 0;
+    fw2v_batch_job_words(b, (int32_t)j, &wr, &wk);
+    printf("Job %zu Words: %llu\n", j + 1, (unsigned long long)wr);
+  }
+  printf("\nOverall Words Per Second: %.4f\n", bs.words_read / (t1 - t0));
+  printf("Overall Words: %llu\nOverall time: %f\n", (unsigned long long)bs.words_read, t1 - t0);
+  for (size_t j = 0; j < opts.size(); j++) {
+    if (!opts[j].do_export) continue;
+    const int d = opts[j].layer_size;
+    std::vector<float> syn0(vocabs[j].counts.size() * (size_t)d);
+    if ((st = fw2v_batch_get_syn0(b, (int32_t)j, syn0.data(), d)) != FW2V_OK) return batch_fail("export", st, b);
+    if (!save_model(opts[j].output, vocabs[j], syn0, d, opts[j].binary)) {
+      fprintf(stderr, "ERROR: cannot write %s\n", opts[j].output.c_str());
+      fw2v_batch_destroy(b);
+      return 1;
+    }
+  }
+  fw2v_batch_destroy(b);
+  return 0;
+}
+
+int main(int argc, char** argv) {
+  Options o;
+  if (!parse(argc, argv, o)) return 0;
+  if (o.debug > 0) {
+    fprintf(stderr, "** FILES & I/O **\n");
+    if (!o.do_export && !o.output.empty()) fprintf(stderr, "!!\tProcess will train but will not export a model!\n");
+    else if (!o.output.empty()) fprintf(stderr, "Trained model will export to file: %s\n", o.output.c_str());
+    else fprintf(stderr, "!!\tPreprocessing only -- no training.\n");
+    fprintf(stderr, "layer size: %d, epochs: %d, alpha: %.5f, window: %d, sample: %f, negative: %d\n",
+            o.layer_size, o.epochs, o.alpha, o.window, o.sample, o.negative);
+  }
+
+  Vocab vocab;
+  Corpus corpus;
+  uint64_t train_words = 0;
+  if (!o.jobs.empty()) return run_jobs(o);
+  if (const int r = prepare(o, vocab, corpus, train_words)) return r < 0 ? 0 : r;
+  const int64_t n_chunks = (int64_t)corpus.chunk_off.size();
+  if (o.pre_shuffle) shuffle_chunks(corpus.chunk_off);
+
+  // InitNet + Train_SGNS through libfw2v
+  const fw2v_config cfg = job_config(o);
   fw2v_handle* h = nullptr;
   fw2v_status st = fw2v_create(&cfg, &h);
   if (st != FW2V_OK) return fail_status("create", st, nullptr);

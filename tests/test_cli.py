@@ -156,3 +156,24 @@ def test_text_export_and_shuffles(tmp_path):
         assert f"Overall Words: {int(g['overall_words'])}" in out
         _, vs = _read_vec(tmp_path / "s.vec")
         assert np.isfinite(vs).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp32", "bf16"])
+def test_jobs_manifest_trains_each_job_as_alone(tmp_path, precision):
+    """-jobs: the jobs of a manifest train together in one batch; with
+    -deterministic 1 each exports the vectors it gets alone (same seed)."""
+    lines = []
+    for i, (name, seed) in enumerate((("zipf_t1", 0), ("messy_t1", 9))):
+        g = load(name)
+        (tmp_path / f"c{i}.txt").write_bytes(g["text"])
+        args = ["-train", f"c{i}.txt", "-output", f"j{i}.vec", "-binary", "1", "-seed", str(seed), "-size",
+                str(16 + 24 * i)] + _flags(g, drop=("-negative", "-size"))
+        lines.append(" ".join(args + ["-negative", "5"]))
+        _run(args + ["-negative", "5", "-output", f"a{i}.vec", "-debug", "0", "-deterministic", "1",
+                     "-precision", precision], tmp_path)
+    (tmp_path / "jobs.txt").write_text("# two jobs\n" + "\n".join(lines) + "\n")
+    out = _run(["-jobs", "jobs.txt", "-deterministic", "1", "-precision", precision], tmp_path)
+    assert "Job 2 Words:" in out and "Overall Words Per Second:" in out
+    for i in range(2):
+        assert (tmp_path / f"j{i}.vec").read_bytes() == (tmp_path / f"a{i}.vec").read_bytes()
