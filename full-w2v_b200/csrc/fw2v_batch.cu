@@ -72,6 +72,7 @@ struct BatchJob {
   std::vector<int64_t> sbase;  // threads + 1: readable-token prefix of its streams
   int64_t gfirst = 0;          // global number of its stream 0
   int lane_vec = 4, lane_nv = 1, stages = 6;
+  int prefetch = 0;  // target rows copied one centre ahead (one group of targets only)
   int family() const { return batch_family(lane_nv, stages); }
 };
 
@@ -240,7 +241,8 @@ void free_plan(fw2v_batch* b) {
 }
 
 int64_t shape_smem_floats(const BatchJob& j) {
-  return (int64_t)WarpRows<1>::rows(2 * j.cfg.window + 1) * j.pitch + 2 * (int64_t)(j.stages - 1) * j.pitch;
+  const bool pre = j.prefetch && j.cfg.negative + 1 <= j.stages;
+  return (int64_t)(2 * j.cfg.window + 1 + 3 + (pre ? 2 : 1) * j.stages) * j.pitch;
 }
 int64_t shape_scratch_elems(const BatchJob& j) { return (int64_t)(2 * j.cfg.window + 1) * j.pitch; }
 
@@ -304,6 +306,7 @@ TrainParams train_params(const fw2v_batch* b, const BatchJob& j, const RoundBuf&
   p.lane_vec = j.lane_vec;
   p.lane_nv = j.lane_nv;
   p.stages = j.stages;
+  p.prefetch = j.prefetch;
   return p;
 }
 
@@ -740,7 +743,8 @@ fw2v_status fw2v_batch_add_job(fw2v_batch* b, const fw2v_config* cfg, const uint
   return FW2V_OK;
 }
 
-fw2v_status fw2v_batch_set_shape(fw2v_batch* b, int32_t job, int32_t lane_vec, int32_t lane_nv, int32_t stages) {
+fw2v_status fw2v_batch_set_shape(fw2v_batch* b, int32_t job, int32_t lane_vec, int32_t lane_nv, int32_t stages,
+                                 int32_t prefetch) {
   if (!b || job < 0 || job >= (int32_t)b->jobs.size()) return bfail(b, FW2V_ERR_ARGUMENT, "bad job");
   BatchJob& j = b->jobs[job];
   if (!valid_shape(j.cfg.layer_size, lane_vec, lane_nv, stages))
@@ -750,15 +754,18 @@ fw2v_status fw2v_batch_set_shape(fw2v_batch* b, int32_t job, int32_t lane_vec, i
   j.lane_vec = lane_vec;
   j.lane_nv = lane_nv;
   j.stages = stages;
+  j.prefetch = prefetch != 0;
   return FW2V_OK;
 }
 
-fw2v_status fw2v_batch_get_shape(fw2v_batch* b, int32_t job, int32_t* lane_vec, int32_t* lane_nv, int32_t* stages) {
-  if (!b || job < 0 || job >= (int32_t)b->jobs.size() || !lane_vec || !lane_nv || !stages)
+fw2v_status fw2v_batch_get_shape(fw2v_batch* b, int32_t job, int32_t* lane_vec, int32_t* lane_nv, int32_t* stages,
+                                 int32_t* prefetch) {
+  if (!b || job < 0 || job >= (int32_t)b->jobs.size() || !lane_vec || !lane_nv || !stages || !prefetch)
     return bfail(b, FW2V_ERR_ARGUMENT, "bad job");
   *lane_vec = b->jobs[job].lane_vec;
   *lane_nv = b->jobs[job].lane_nv;
   *stages = b->jobs[job].stages;
+  *prefetch = b->jobs[job].prefetch;
   return FW2V_OK;
 }
 
@@ -1024,25 +1031,30 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
     const int def_vec = j0.pitch <= 64 ? 2 : 4, def_nv = j0.pitch <= 128 ? 1 : (j0.pitch <= 256 ? 2 : 3);
     const int def_st = default_stages(b->negative, def_nv);
     double best = -1, def_wps = 0;
-    int best_vec = def_vec, best_nv = def_nv, best_st = def_st;
+    int best_vec = def_vec, best_nv = def_nv, best_st = def_st, best_pre = 0;
     for (int vec : {2, 4}) {
       for (int st : kBatchStages) {
-        if (result != FW2V_OK || !valid_shape(d_max, vec, def_nv, st)) continue;
-        for (int j : members[c]) {
-          b->jobs[j].lane_vec = vec;
-          b->jobs[j].lane_nv = def_nv;
-          b->jobs[j].stages = st;
-        }
-        float ms = 0;
-        const int fam = batch_family(def_nv, st);
-        result = time_round(b, r, members[c], fam, b->warps_per_block[fam], b->blocks_per_sm[fam], 2, &ms);
-        if (result != FW2V_OK) break;
-        const double wps = kept / (ms / 1e3);
-        if (vec == def_vec && st == def_st) def_wps = wps;
-        if (wps > best) {
-          best = wps;
-          best_vec = vec;
-          best_st = st;
+        for (int pre : {0, 1}) {
+          if (result != FW2V_OK || !valid_shape(d_max, vec, def_nv, st)) continue;
+          if (pre && b->negative + 1 > st) continue;  // the prefetch needs all targets in one group
+          for (int j : members[c]) {
+            b->jobs[j].lane_vec = vec;
+            b->jobs[j].lane_nv = def_nv;
+            b->jobs[j].stages = st;
+            b->jobs[j].prefetch = pre;
+          }
+          float ms = 0;
+          const int fam = batch_family(def_nv, st);
+          result = time_round(b, r, members[c], fam, b->warps_per_block[fam], b->blocks_per_sm[fam], 2, &ms);
+          if (result != FW2V_OK) break;
+          const double wps = kept / (ms / 1e3);
+          if (vec == def_vec && st == def_st && !pre) def_wps = wps;
+          if (wps > best) {
+            best = wps;
+            best_vec = vec;
+            best_st = st;
+            best_pre = pre;
+          }
         }
       }
     }
@@ -1050,12 +1062,14 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
       b->jobs[j].lane_vec = best_vec;
       b->jobs[j].lane_nv = best_nv;
       b->jobs[j].stages = best_st;
+      b->jobs[j].prefetch = best_pre;
     }
     rep.class_d[c] = d_max;
     rep.class_window[c] = keys[c].second;
     rep.class_lane_vec[c] = best_vec;
     rep.class_lane_nv[c] = best_nv;
     rep.class_stages[c] = best_st;
+    rep.class_prefetch[c] = best_pre;
     rep.tuned_wps[c] = best;
     rep.default_wps[c] = def_wps;
     bfree(r.dev);

@@ -68,19 +68,16 @@ __host__ __device__ __forceinline__ uint64_t sr_event_key(uint64_t skey, uint64_
 }
 __host__ __device__ __forceinline__ uint64_t sr_vector_bits(uint64_t key, uint64_t row, uint64_t vec) {
   const uint32_t lo = fmix32((uint32_t)key ^ ((uint32_t)row * 0x27D4EB2Fu) ^ ((uint32_t)vec * 0x165667B1u));
-  const uint32_t hi = fmix32(lo ^ (uint32_t)(key >> 32));
+  uint32_t hi = (lo ^ (uint32_t)(key >> 32)) * 0x9E3779B9u;
+  hi ^= hi >> 15;
   return ((uint64_t)hi << 32) | lo;
 }
-// x rounded to bfloat16 up or down with probability proportional to the
-// distance (r16 uniform in [0, 65536)); NaN and infinity round to nearest.
-__host__ __device__ __forceinline__ uint16_t bf16_stochastic(float x, uint32_t r16) {
-  uint32_t b;
-  memcpy(&b, &x, 4);
-  if ((b & 0x7F800000u) == 0x7F800000u) {
-    if (b & 0x007FFFFFu) return (uint16_t)((b >> 16) | 0x40);  // quiet NaN
-    return (uint16_t)(b >> 16);                                // infinity
-  }
-  return (uint16_t)((b + (r16 & 0xFFFFu)) >> 16);
+// x (finite) rounded to bfloat16 up or down in magnitude with probability
+// equal to its distance from the truncated value, widened back to float: 16
+// random bits r16 (uniform in [0, 65536)) carry into the kept bits and the 16
+// discarded bits are cleared.
+__device__ __forceinline__ float bf16_stochastic_value(float x, uint32_t r16) {
+  return __uint_as_float((__float_as_uint(x) + r16) & 0xFFFF0000u);
 }
 __host__ __device__ __forceinline__ float bf16_value(uint16_t h) {
   const uint32_t b = (uint32_t)h << 16;
@@ -214,6 +211,7 @@ struct TrainParams {
   int64_t scratch_warps;
   uint64_t sr_seed;  // stochastic rounding of bfloat16 write-backs
   int bf16;          // tables hold bfloat16
+  int prefetch;      // copy each centre's target rows while the previous centre trains
   // batched launches: lane vector width (2 or 4), vectors per lane (1 to 3)
   // and pipeline stages of this job's sentences
   int lane_vec, lane_nv, stages;

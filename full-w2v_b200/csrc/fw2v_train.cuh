@@ -273,8 +273,8 @@ __device__ __forceinline__ void row_load_global(Row<VEC, NV>& r, const bf16_t* r
 // no other writer touched the row since the load, the stored value becomes s
 // exactly.  Concurrent writers never lose each other's updates.
 __device__ __forceinline__ uint32_t sr_increment2(float a0, float b0, float a1, float b1, uint32_t r32) {
-  const float x0 = __fsub_rn(bf16_value(bf16_stochastic(a0, r32 & 0xFFFFu)), b0);
-  const float x1 = __fsub_rn(bf16_value(bf16_stochastic(a1, r32 >> 16)), b1);
+  const float x0 = __fsub_rn(bf16_stochastic_value(a0, r32 & 0xFFFFu), b0);
+  const float x1 = __fsub_rn(bf16_stochastic_value(a1, r32 >> 16), b1);
   const __nv_bfloat162 v = __floats2bfloat162_rn(x0, x1);  // x0 in the low half (lower address)
   return *reinterpret_cast<const uint32_t*>(&v);
 }
@@ -301,7 +301,7 @@ __device__ __forceinline__ void row_add_delta(bf16_t* row, const Row<VEC, NV>& a
       for (int j = 0; j < VEC; j++) {
         if (e + j >= d) continue;
         const uint32_t r16 = (uint32_t)(bits >> (16 * j)) & 0xFFFFu;
-        const float x = __fsub_rn(bf16_value(bf16_stochastic(a.x[i][j], r16)), b.x[i][j]);
+        const float x = __fsub_rn(bf16_stochastic_value(a.x[i][j], r16), b.x[i][j]);
         const __nv_bfloat16 v = __float2bfloat16_rn(x);
         const unsigned short u = *reinterpret_cast<const unsigned short*>(&v);
         asm volatile("red.global.add.noftz.bf16 [%0], %1;" ::"l"(h + e + j), "h"(u) : "memory");
@@ -563,12 +563,12 @@ __device__ __forceinline__ void lds_staged(Row<VEC, NV>& r, uint32_t row, const 
 // Shared-memory rows of one warp, each `P` floats.
 template <int R>
 struct WarpRows {
-  static constexpr int kExtra = 1 + 2 * R + 2;  // sink, 2 x R target rows, 2 staging rows
-  __host__ __device__ static constexpr int rows(int D) { return D + kExtra; }
+  // ring, sink, R target rows (2 x R with the target prefetch), 2 staging rows
+  __host__ __device__ static constexpr int rows(int D, bool prefetch) { return D + 1 + (prefetch ? 2 : 1) * R + 2; }
 };
 
 // One sentence on one warp.
-//   ring     shared memory (WarpRows<R>::rows(D) rows): slot p % D holds the
+//   ring     shared memory (WarpRows<R>::rows rows): slot p % D holds the
 //            current value of sentence position p while it is in the window;
 //            slot D is a sink that the pipeline reads and writes on its idle
 //            steps; then the R target rows as loaded (for their write-back) and
@@ -590,6 +590,7 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   T* const syn1neg = reinterpret_cast<T*>(p.syn1neg);
   const float alpha = sn.alpha;
   const bool one_group = K + 1 <= R;
+  const bool pre = one_group && p.prefetch;  // target rows copied one centre ahead
   const uint64_t skey = sr_sentence_key(p.sr_seed, (uint64_t)sn.uid);  // bfloat16 tables only
 
   // Every id is checked before any table access.
@@ -619,14 +620,14 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   const uint32_t ring_b = smem_addr(ring);
   const uint32_t row_bytes = (uint32_t)P * 4u;
   const uint32_t sink_b = ring_b + (uint32_t)D * row_bytes;
-  // Target rows: two sets of R rows.  With all 1 + K targets of a centre in
-  // one group, centre w's rows were copied (cp.async, table element type)
-  // into set w % 2 while centre w-1 trained, and are kept there as the
-  // originals for the write-back; otherwise set 0 holds the FP32 originals of
-  // the current group.
+  // Target rows.  With the prefetch (all 1 + K targets of a centre in one
+  // group), two sets of R rows: centre w's rows were copied (cp.async, table
+  // element type) into set w % 2 while centre w-1 trained, and stay there as
+  // the originals for the write-back.  Otherwise one set holds the FP32
+  // originals of the current group, loaded when it starts.
   const uint32_t o0_b = sink_b + row_bytes;
   const uint32_t o1_b = o0_b + (uint32_t)R * row_bytes;
-  const uint32_t in_b = o1_b + (uint32_t)R * row_bytes;
+  const uint32_t in_b = pre ? o1_b + (uint32_t)R * row_bytes : o1_b;
   const uint32_t out_b = in_b + row_bytes;
   auto prefetch_targets = [&](uint32_t set, int my_target) {
     for (int k = 0; k <= K; k++) {
@@ -647,7 +648,7 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   }
 
   int t_next = one_group ? target_id(ids, negs, K, 0, 0, K + 1, lane) : 0;
-  if (one_group) {
+  if (pre) {
     prefetch_targets(o0_b, t_next);
     cp_async_commit();
     cp_async_wait();
@@ -662,7 +663,7 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
     const uint32_t cur_b = (w & 1) ? o1_b : o0_b;
     if (one_group && w + 1 < L) {
       t_next = target_id(ids, negs, K, w + 1, 0, K + 1, lane);
-      prefetch_targets((w & 1) ? o0_b : o1_b, t_next);
+      if (pre) prefetch_targets((w & 1) ? o0_b : o1_b, t_next);
     }
     // The entering row can be fetched now unless the leaving position holds
     // the same word (its write-back must land first).  Both staging copies run
@@ -698,7 +699,7 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
           for (int k = 0; k < R; k++) {
             const int tk = __shfl_sync(kFull, my_t, k);
             if (k < nt) {
-              if (one_group) {
+              if (pre) {
                 // The copy was taken before the previous centre's write-back:
                 // a target it also wrote is fetched again (after this lane's
                 // own reduction, in program order).
@@ -760,7 +761,7 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
             const int tk = __shfl_sync(kFull, my_t, k);
             if (k < nt) {
               Row<VEC, NV> o0;
-              if (one_group) lds_staged<T>(o0, cur_b + (uint32_t)k * row_bytes, lm);
+              if (pre) lds_staged<T>(o0, cur_b + (uint32_t)k * row_bytes, lm);
               else lds_row(o0, o0_b + (uint32_t)k * row_bytes, lm);
               row_add_delta(syn1neg + (int64_t)tk * P, o[k], o0, lane, d,
                             sr_event_key(skey, (uint64_t)w * (K + 1) + (k0 + k)),
@@ -846,7 +847,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MinBlocks<NV>::value) sgn
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int D = 2 * p.window + 1;
-  float* ring = smem + (int64_t)warp * WarpRows<R>::rows(D) * p.pitch;
+  float* ring = smem + (int64_t)warp * WarpRows<R>::rows(D, p.prefetch && p.negative + 1 <= R) * p.pitch;
   const int64_t gwarp = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
   T* orig = reinterpret_cast<T*>(p.orig_scratch) + gwarp * D * p.pitch;
   const int64_t total = total_sentences(p);

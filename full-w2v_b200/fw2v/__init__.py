@@ -61,7 +61,8 @@ class BatchStats(C.Structure):
 class TuneReport(C.Structure):
     _fields_ = [("n_classes", C.c_int32), ("class_d", C.c_int32 * 16), ("class_window", C.c_int32 * 16),
                 ("class_lane_vec", C.c_int32 * 16), ("class_lane_nv", C.c_int32 * 16),
-                ("class_stages", C.c_int32 * 16), ("tuned_wps", C.c_double * 16),
+                ("class_stages", C.c_int32 * 16), ("class_prefetch", C.c_int32 * 16),
+                ("tuned_wps", C.c_double * 16),
                 ("default_wps", C.c_double * 16), ("warps_per_block", C.c_int32 * 3),
                 ("blocks_per_sm", C.c_int32 * 3)]
 
@@ -134,8 +135,9 @@ def lib() -> C.CDLL:
             "fw2v_batch_last_error": (C.c_char_p, [H]),
             "fw2v_batch_add_job": (C.c_int, [H, C.POINTER(Config), P, I64, U64, P, I64, P, I64,
                                              C.POINTER(I32)]),
-            "fw2v_batch_set_shape": (C.c_int, [H, I32, I32, I32, I32]),
-            "fw2v_batch_get_shape": (C.c_int, [H, I32, C.POINTER(I32), C.POINTER(I32), C.POINTER(I32)]),
+            "fw2v_batch_set_shape": (C.c_int, [H, I32, I32, I32, I32, I32]),
+            "fw2v_batch_get_shape": (C.c_int, [H, I32, C.POINTER(I32), C.POINTER(I32), C.POINTER(I32),
+                                               C.POINTER(I32)]),
             "fw2v_batch_set_launch": (C.c_int, [H, I32, I32, I32]),
             "fw2v_batch_get_launch": (C.c_int, [H, I32, C.POINTER(I32), C.POINTER(I32)]),
             "fw2v_batch_tune": (C.c_int, [H, I64, C.POINTER(TuneReport)]),
@@ -391,14 +393,16 @@ class Batch:
         self.jobs.append((config, len(counts)))
         return j.value
 
-    def set_shape(self, job: int, lane_vec: int, lane_nv: int, stages: int):
-        self._check(lib().fw2v_batch_set_shape(self._h, job, lane_vec, lane_nv, stages), "batch_set_shape")
+    def set_shape(self, job: int, lane_vec: int, lane_nv: int, stages: int, prefetch: int = 0):
+        self._check(lib().fw2v_batch_set_shape(self._h, job, lane_vec, lane_nv, stages, prefetch),
+                    "batch_set_shape")
 
-    def shape(self, job: int) -> tuple[int, int, int]:
-        v, n, s = C.c_int32(), C.c_int32(), C.c_int32()
-        self._check(lib().fw2v_batch_get_shape(self._h, job, C.byref(v), C.byref(n), C.byref(s)),
+    def shape(self, job: int) -> tuple[int, int, int, int]:
+        """(lane vector width, vectors per lane, stages, prefetch)."""
+        v, n, s, p = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        self._check(lib().fw2v_batch_get_shape(self._h, job, C.byref(v), C.byref(n), C.byref(s), C.byref(p)),
                     "batch_get_shape")
-        return v.value, n.value, s.value
+        return v.value, n.value, s.value, p.value
 
     def set_launch(self, family: int, warps_per_block: int, blocks_per_sm: int = 0):
         self._check(lib().fw2v_batch_set_launch(self._h, family, warps_per_block, blocks_per_sm),
@@ -434,7 +438,8 @@ class Batch:
         for c in range(rep.n_classes):
             out["classes"].append({"d": rep.class_d[c], "window": rep.class_window[c],
                                    "lane_vec": rep.class_lane_vec[c], "lane_nv": rep.class_lane_nv[c],
-                                   "stages": rep.class_stages[c], "tuned_wps": rep.tuned_wps[c],
+                                   "stages": rep.class_stages[c], "prefetch": rep.class_prefetch[c],
+                                   "tuned_wps": rep.tuned_wps[c],
                                    "default_wps": rep.default_wps[c]})
         if cache:
             for j, k in enumerate(keys):

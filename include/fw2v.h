@@ -284,12 +284,16 @@ fw2v_status fw2v_batch_add_job(fw2v_batch* b, const fw2v_config* cfg, const uint
 
 /* A job's kernel shape: the lane vector width and vectors per lane (2 x 1:
  * 32 lanes of 2 floats cover d <= 64; 4 x 1: d <= 128, 16 lanes suffice for
- * d <= 64; 4 x 2: d <= 256; 4 x 3: d <= 384) and the pipeline stages (2, 3, 4
- * or 6 targets in flight).  Defaults follow d and negative; fw2v_batch_tune
- * picks them by measurement. */
-fw2v_status fw2v_batch_set_shape(fw2v_batch* b, int32_t job, int32_t lane_vec, int32_t lane_nv, int32_t stages);
+ * d <= 64; 4 x 2: d <= 256; 4 x 3: d <= 384), the pipeline stages (2, 3, 4
+ * or 6 targets in flight; 4 at most with 3 vectors per lane) and the target
+ * prefetch (1: each centre's target rows are copied into shared memory while
+ * the previous centre trains; used when all 1 + negative targets fit one
+ * group of stages).  Defaults follow d and negative, prefetch off;
+ * fw2v_batch_tune picks them by measurement. */
+fw2v_status fw2v_batch_set_shape(fw2v_batch* b, int32_t job, int32_t lane_vec, int32_t lane_nv, int32_t stages,
+                                 int32_t prefetch);
 fw2v_status fw2v_batch_get_shape(fw2v_batch* b, int32_t job, int32_t* lane_vec, int32_t* lane_nv,
-                                 int32_t* stages);
+                                 int32_t* stages, int32_t* prefetch);
 
 /* The training grid of a kernel family (0: one vector per lane; 1: wide rows
  * with 2 or 3 stages (2 vectors per lane) or 2 stages (3 vectors); 2: other
@@ -308,6 +312,7 @@ fw2v_status fw2v_batch_get_launch(fw2v_batch* b, int32_t family, int32_t* warps_
 typedef struct fw2v_batch_tune_report {
   int32_t n_classes;
   int32_t class_d[16], class_window[16], class_lane_vec[16], class_lane_nv[16], class_stages[16];
+  int32_t class_prefetch[16];
   double tuned_wps[16], default_wps[16];
   int32_t warps_per_block[3], blocks_per_sm[3];  /* per kernel family */
 } fw2v_batch_tune_report;

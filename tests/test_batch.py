@@ -127,8 +127,9 @@ def test_deterministic_batch_equals_each_job_alone_bf16(jobs):
             np.testing.assert_array_equal(b.syn1neg(j), r1[:, :over["layer_size"]])
 
 
-SHAPES = ([(2, (2, 1, s)) for s in (2, 3, 4, 6)] + [(2, (4, 1, s)) for s in (2, 3, 4, 6)] +
-          [(5, (4, 2, s)) for s in (2, 3, 4, 6)] + [(6, (4, 3, s)) for s in (2, 3, 4)])
+SHAPES = ([(2, (2, 1, s, 0)) for s in (2, 3, 4, 6)] + [(2, (4, 1, s, 0)) for s in (2, 3, 4, 6)] +
+          [(5, (4, 2, s, 0)) for s in (2, 3, 4, 6)] + [(6, (4, 3, s, 0)) for s in (2, 3, 4)] +
+          [(2, (2, 1, 6, 1)), (2, (4, 1, 6, 1)), (5, (4, 2, 6, 1)), (3, (4, 1, 6, 1))])
 
 
 @pytest.mark.parametrize("job,shape", SHAPES)
@@ -145,7 +146,7 @@ def test_every_shape_trains_bit_exact(jobs, job, shape):
 def test_batch_job_equals_single_job_handle(jobs):
     corpus, over = jobs[3]
     with _batch([(corpus, over)], deterministic=True) as b:
-        b.set_shape(0, 4, 1, 6)  # the single-job kernel's layout for d = 100 and negative 5
+        b.set_shape(0, 4, 1, 6, 0)  # the single-job kernel's layout for d = 100 and negative 5
         b.train()
         got0, got1 = b.syn0(0), b.syn1neg(0)
     with fw2v.Trainer(_config(dict(over, deterministic=1))) as t:
@@ -194,7 +195,7 @@ def test_tuner_picks_valid_shapes_and_restores_state(jobs):
         assert rep["classes"] and all(c["tuned_wps"] >= c["default_wps"] > 0 for c in rep["classes"])
         for j, (corpus, over) in enumerate(jobs):
             np.testing.assert_array_equal(b.syn0(j), before[j])
-            vec, nv, st = b.shape(j)
+            vec, nv, st, _ = b.shape(j)
             assert st in (2, 3, 4, 6) and vec * nv * 32 >= over["layer_size"]
         st = b.train()  # sampler state was restored: the same words as never tuned
         assert st.words_read == sum(_words(c, o) for c, o in jobs)
@@ -221,7 +222,7 @@ def test_batch_rejects_bad_jobs(jobs):
         with pytest.raises(fw2v.Fw2vError):
             b.add_job(fw2v.default_config(negative=3, **{k: v for k, v in over.items()}), corpus.counts,
                       corpus.train_words, corpus.stream, corpus.chunk_off)
-        for bad_shape in ((2, 1, 5), (4, 2, 6), (2, 2, 4)):  # no such stages; d = 8 needs one vector; 2-float wide
+        for bad_shape in ((2, 1, 5, 0), (4, 2, 6, 0), (2, 2, 4, 0)):  # stages; d = 8 needs one vector; 2-float wide
             with pytest.raises(fw2v.Fw2vError):
                 b.set_shape(0, *bad_shape)
         bad = corpus.stream.copy()
