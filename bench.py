@@ -189,10 +189,20 @@ def cpu_baseline(corpus, cfg, threads, seconds_target=15.0):
 def make_corpus(args):
     """(corpus, held-out stream or None, config) of the workload: the numpy
     generator for c1/c2 (the reference program reads the same corpus as text),
-    the device generator for c3 (800M tokens)."""
+    the device generators for c3 (800M tokens) and c4 (walks on a 1M-node
+    graph, 800M tokens)."""
     from fw2v import synth
     if args.config == "c3":
         return synth.make_topic_corpus_gpu(args.config, n_tokens=args.tokens, heldout_tokens=args.heldout)
+    if args.config == "c4":
+        g = dict(synth.GRAPH_CONFIGS["c4"])
+        if args.tokens:
+            g["nodes"] = max(1000, args.tokens // (g["walks_per_node"] * (g["walk_len"] + 1)))
+        corpus, held = synth.sbm_corpus_gpu(g["nodes"], g["blocks"], g["degree"], g["p_ratio"],
+                                            g["walks_per_node"], g["walk_len"], seed=1234 + 4,
+                                            heldout_walks=max(1, args.heldout // (g["walk_len"] + 1)))
+        cfg = dict(g, n_tokens=len(corpus.stream) - 1, min_count=1)
+        return corpus, held, cfg
     corpus, cfg = synth.make_topic_corpus(args.config, n_tokens=args.tokens)
     return corpus, None, cfg
 
@@ -298,6 +308,9 @@ def run_own(args, world, rank, local):
     total_s = max_over_ranks(world, sum(r[2] for r in res) / 1e3)
     value = sum_over_ranks(world, float(words)) / total_s
     loss = heldout(fw2v.Trainer, corpus, cfg, pairs, syn0, syn1) if pairs is not None else None
+    p10 = None
+    if corpus.purity is not None:
+        p10, _ = evaluate.precision_at_10(syn0, corpus.label, corpus.counts, purity=corpus.purity, device=dev)
     del syn0, syn1
 
     # e2e: through the public API from pinned host buffers, every step
@@ -350,10 +363,14 @@ def run_own(args, world, rank, local):
             e1.synchronize()
             ms += e0.elapsed_time(e1)
         cval = sum_over_ranks(world, float(cw)) / max_over_ranks(world, ms / 1e3)
-        closs = heldout(fw2v.Trainer, corpus, cfg, pairs, tr.syn0(), tr.syn1neg()) if pairs is not None else None
+        cs0 = tr.syn0()
+        closs = heldout(fw2v.Trainer, corpus, cfg, pairs, cs0, tr.syn1neg()) if pairs is not None else None
+        cp10 = None
+        if corpus.purity is not None:
+            cp10, _ = evaluate.precision_at_10(cs0, corpus.label, corpus.counts, purity=corpus.purity, device=dev)
         tr.close()
         compare = {"form": "fp32 (single-job kernel, untuned)", "value": cval, "unit": UNIT,
-                   "epochs_timed": min(args.steps, 2), "heldout_loss": closs,
+                   "epochs_timed": min(args.steps, 2), "heldout_loss": closs, "precision_at_10": cp10,
                    "speedup": value / cval,
                    "heldout_loss_rel_diff": (loss - closs) / closs if loss is not None and closs else None}
 
@@ -377,8 +394,10 @@ def run_own(args, world, rank, local):
         "warmup": args.warmup, "ms_per_step": epoch_ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "bf16-tables/f32-math" if bf16 else "f32",
-        "data": "synthetic (seeded topic-mixture corpus, generated in-process)",
-        "config": {"workload": f"{args.config}: {(args.tokens or cfg['n_tokens'])/1e6:.0f}M-token topic corpus, "
+        "data": "synthetic (seeded " + ("random walks on a stochastic block model" if args.config == "c4"
+                                         else "topic-mixture corpus") + ", generated in-process)",
+        "config": {"workload": f"{args.config}: {cfg['n_tokens']/1e6:.0f}M-token "
+                               f"{'walk' if args.config == 'c4' else 'topic'} corpus, "
                                f"V={len(corpus.counts)}, d={d}, window={W}, negative={K}, sample={cfg['sample']}, "
                                f"msl=1000, {T} sampling streams; form {form}",
                    "form": form, "tokens_per_epoch": int(len(corpus.stream) - 1), "vocab": len(corpus.counts),
@@ -388,6 +407,7 @@ def run_own(args, world, rank, local):
                    "l2": "flushed between steps (256 MB write, untimed); tables exceed L2"
                          if args.config == "c3" else "flushed between steps (256 MB write, untimed)"},
         "heldout_loss": loss,
+        "precision_at_10": p10,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
         "gpu_launches": int(sum(r[3] for r in res)),
@@ -408,6 +428,77 @@ def run_own(args, world, rank, local):
     return out
 
 
+def run_c5(args, world, rank, local):
+    """The batched configuration: 256 independent graph jobs (synth.c5_job_specs,
+    node counts times --scale).  Each job is generated on the device, trained
+    alone with the plain FP32 single-job kernel (timed, scored), then added to
+    one batch that trains all of them in the value's form (tuned, one CUDA
+    graph).  value = words of all jobs / the batch's device time; fp32_alone =
+    the same words / the sum of the jobs' own device times."""
+    import torch
+
+    import fw2v
+    from fw2v import evaluate, synth
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    specs = synth.c5_job_specs(scale=args.scale)
+    prec = fw2v.BF16 if args.form.startswith("bf16") else fw2v.FP32
+    batch = fw2v.Batch(precision=prec, device=local)
+    labels, alone_p10, alone_ms, alone_words = [], [], 0.0, 0
+    for j, s in enumerate(specs):
+        corpus, _ = synth.sbm_corpus_gpu(s["nodes"], s["blocks"], s["degree"], s["p_ratio"], s["walks_per_node"],
+                                         s["walk_len"], seed=s["seed"])
+        T = default_streams(len(corpus.chunk_off))
+        cfg = fw2v.default_config(layer_size=s["d"], window=s["window"], negative=s["negative"], epochs=s["epochs"],
+                                  threads=T, msl=1000, alpha=0.025, sample=s["sample"], seed=s["seed"])
+        if not args.no_compare:
+            with fw2v.Trainer(cfg) as t:
+                t.set_vocab(corpus.counts, corpus.train_words)
+                t.load_corpus(corpus.stream, corpus.chunk_off)
+                ts = torch.cuda.ExternalStream(t.stream_handle(), device=dev)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(ts)
+                alone_words += t.train()
+                e1.record(ts)
+                e1.synchronize()
+                alone_ms += e0.elapsed_time(e1)
+                alone_p10.append(evaluate.precision_at_10(t.syn0(), corpus.label, corpus.counts,
+                                                          purity=corpus.purity, device=dev)[0])
+        batch.add_job(cfg, corpus.counts, corpus.train_words, corpus.stream, corpus.chunk_off)
+        labels.append((corpus.label, corpus.counts, corpus.purity))
+        del corpus
+    tuned = batch.tune()
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize(dev)
+        st = batch.train()
+        torch.cuda.synchronize(dev)
+    value = st.words_read / (st.ms / 1e3)
+    p10 = [evaluate.precision_at_10(batch.syn0(j), *labels[j][:2], purity=labels[j][2], device=dev)[0]
+           for j in range(len(specs))]
+    batch.close()
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": 1, "warmup": 0,
+           "ms_per_step": st.ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "bf16-tables/f32-math" if prec == fw2v.BF16 else "f32",
+           "data": "synthetic (seeded random walks on 256 stochastic block models, generated in-process)",
+           "config": {"workload": f"c5: {len(specs)} graph jobs, {st.words_read / 1e9:.2f}B tokens, one batch; "
+                                  f"form {args.form}", "form": args.form, "jobs": len(specs), "scale": args.scale,
+                      "rounds": st.rounds, "tuning": tuned},
+           "precision_at_10": {"mean": float(np.nanmean(p10)), "min": float(np.nanmin(p10))},
+           "gpu_launches": 5 * st.rounds}
+    if alone_p10:
+        diff = np.array(p10) - np.array(alone_p10)
+        out["fp32_alone"] = {"form": "each job alone, fp32 single-job kernel", "value": alone_words / (alone_ms / 1e3),
+                             "unit": UNIT, "speedup": value / (alone_words / (alone_ms / 1e3)),
+                             "precision_at_10_mean": float(np.nanmean(alone_p10)),
+                             "p10_diff_mean": float(np.nanmean(diff)), "p10_diff_min": float(np.nanmin(diff)),
+                             "jobs_within_1_point": int(np.sum(diff >= -0.01))}
+    clocks = clk.summary()
+    if clocks:
+        out["clocks"] = clocks
+    return out
+
+
 def run_reference(args, world, rank):
     """The reference program (oracle/_ref/FULL-W2V) on the same corpus, or the
     CPU port where it cannot run."""
@@ -416,12 +507,17 @@ def run_reference(args, world, rank):
 
     if world > 1 and rank != 0:
         return None
+    if args.config == "c5":
+        return {"impl": "reference", "unavailable": "the reference trains one corpus per process; the batched "
+                                                    "configuration has no reference form (use --config c3)"}
     corpus, _, cfg = make_corpus(args)
     T_stream = args.streams or default_streams(len(corpus.chunk_off))
     cores = os.cpu_count() or 1
     binary = os.path.join(ROOT, "oracle", "_ref", "FULL-W2V")
     reason = None
-    if cfg["d"] > 256 or cfg["d"] % 32:
+    if args.config not in ("c1", "c2"):
+        reason = f"{args.config} is generated on the device and is not written as text for the reference program"
+    elif cfg["d"] > 256 or cfg["d"] % 32:
         reason = f"reference kernel unsupported at d={cfg['d']} (shared-memory overlap / partial warp)"
     elif not os.path.exists(binary):
         reason = "oracle/_ref/FULL-W2V not built"
@@ -519,7 +615,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fw2v", choices=["fw2v", "reference"])
-    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3"])
+    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--scale", type=float, default=1.0, help="c5: node counts of the jobs times this")
     ap.add_argument("--tokens", type=int, default=None, help="override the corpus size")
     ap.add_argument("--streams", type=int, default=None, help="sampling streams (-threads)")
     ap.add_argument("--form", default="bf16-batched", choices=["bf16-batched", "fp32-batched", "bf16", "fp32"],
@@ -532,6 +629,8 @@ def main():
     world, rank, local = dist_setup()
     if args.impl == "reference":
         out = run_reference(args, world, rank)
+    elif args.config == "c5":
+        out = run_c5(args, world, rank, local)
     else:
         out = run_own(args, world, rank, local)
     if rank == 0 and out is not None:

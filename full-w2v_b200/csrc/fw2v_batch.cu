@@ -172,6 +172,18 @@ struct fw2v_batch {
   int64_t scratch_elems = 0, scratch_warps = 0, scratch_bytes = 0;
   int warps_per_block[kBatchFamilies] = {4, 4, 4}, blocks_per_sm[kBatchFamilies] = {0, 0, 0};  // per family
   int epochs_run = 0;  // batch epochs trained so far: job j has trained min(epochs_run, its epochs)
+  // The first round of the next epoch may already be sampled (by the end of
+  // the previous train call, while the host returns) into buf[next_buf];
+  // pre_* hold the state from before that sampling, to undo it.
+  int next_buf = 0;
+  bool presampled = false;
+  uint64_t* pre_lcg = nullptr;
+  uint64_t* pre_wca = nullptr;
+  float* pre_alpha = nullptr;
+  int64_t* pre_uid = nullptr;
+  unsigned long long* pre_words = nullptr;
+  unsigned long long* pre_kept = nullptr;
+  std::vector<unsigned long long> words_snap, kept_snap;  // counters at the end of the last call
 };
 
 namespace {
@@ -310,10 +322,14 @@ TrainParams train_params(const fw2v_batch* b, const BatchJob& j, const RoundBuf&
   return p;
 }
 
+fw2v_status cancel_presample(fw2v_batch* b);
+
 // The round plan of an epoch and buffers for its largest round.
 fw2v_status plan(fw2v_batch* b) {
   if (b->planned) return FW2V_OK;
   if (b->jobs.empty()) return bfail(b, FW2V_ERR_STATE, "batch has no jobs");
+  const fw2v_status pre = cancel_presample(b);  // its round and buffer are about to go
+  if (pre != FW2V_OK) return pre;
   free_plan(b);
   struct Item {
     int32_t job, local;
@@ -493,14 +509,19 @@ cudaError_t enqueue_epochs(fw2v_batch* b, int e0, int epochs, const Grid* grids)
   if (e == cudaSuccess) e = cudaStreamWaitEvent(b->sst, b->ev_fork, 0);
   int64_t k = 0;
   for (int ep = e0; ep < e0 + epochs && e == cudaSuccess; ep++) {
-    e = cudaMemsetAsync(b->job_uid, 0, b->jobs.size() * sizeof(int64_t), b->sst);
+    // the first round sampled ahead: its sampling (and the training stream's
+    // wait for it) happened before this sequence
+    const bool ahead = ep == e0 && b->presampled;
+    if (!ahead) e = cudaMemsetAsync(b->job_uid, 0, b->jobs.size() * sizeof(int64_t), b->sst);
     for (size_t ri = 0; ri < b->rounds.size() && e == cudaSuccess; ri++, k++) {
-      RoundBuf& rb = b->buf[k % 2];
+      RoundBuf& rb = b->buf[(b->next_buf + k) % 2];
       const RoundPlan& r = b->rounds[ri];
-      if (k >= 2) e = cudaStreamWaitEvent(b->sst, rb.freed, 0);
-      if (e == cudaSuccess) e = enqueue_sample(b, rb, r.view, r.max_region, ep);
-      if (e == cudaSuccess) e = cudaEventRecord(rb.ready, b->sst);
-      if (e == cudaSuccess) e = cudaStreamWaitEvent(b->st, rb.ready, 0);
+      if (!(ahead && ri == 0)) {
+        if (k >= 2) e = cudaStreamWaitEvent(b->sst, rb.freed, 0);
+        if (e == cudaSuccess) e = enqueue_sample(b, rb, r.view, r.max_region, ep);
+        if (e == cudaSuccess) e = cudaEventRecord(rb.ready, b->sst);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->st, rb.ready, 0);
+      }
       if (e == cudaSuccess) e = cudaMemsetAsync(b->counter, 0, sizeof(unsigned long long), b->st);
       const Grid& g = grids[r.family];
       if (e == cudaSuccess) e = launch_train_round(b, r.family, train_args(b, rb, r.view, ep, g), g, b->st);
@@ -510,6 +531,50 @@ cudaError_t enqueue_epochs(fw2v_batch* b, int e0, int epochs, const Grid* grids)
   if (e == cudaSuccess) e = cudaEventRecord(b->ev_join, b->sst);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(b->st, b->ev_join, 0);
   return e;
+}
+
+// Sample the first round of epoch `ep` into buf[next_buf] on the sampler
+// stream (not waited for), keeping the state it changes to undo it.
+fw2v_status presample(fw2v_batch* b, int ep) {
+  const size_t J = b->jobs.size();
+  const int64_t G = b->n_gstreams;
+  if (!b->pre_lcg) {
+    BCK(b, balloc(b->pre_lcg, G));
+    BCK(b, balloc(b->pre_wca, G));
+    BCK(b, balloc(b->pre_alpha, G));
+    BCK(b, balloc(b->pre_uid, J));
+    BCK(b, balloc(b->pre_words, J));
+    BCK(b, balloc(b->pre_kept, J));
+  }
+  BCK(b, cudaMemcpyAsync(b->pre_lcg, b->lcg, G * 8, cudaMemcpyDeviceToDevice, b->sst));
+  BCK(b, cudaMemcpyAsync(b->pre_wca, b->wca, G * 8, cudaMemcpyDeviceToDevice, b->sst));
+  BCK(b, cudaMemcpyAsync(b->pre_alpha, b->alpha, G * 4, cudaMemcpyDeviceToDevice, b->sst));
+  BCK(b, cudaMemcpyAsync(b->pre_uid, b->job_uid, J * 8, cudaMemcpyDeviceToDevice, b->sst));
+  BCK(b, cudaMemcpyAsync(b->pre_words, b->job_words, J * 8, cudaMemcpyDeviceToDevice, b->sst));
+  BCK(b, cudaMemcpyAsync(b->pre_kept, b->job_kept, J * 8, cudaMemcpyDeviceToDevice, b->sst));
+  RoundBuf& rb = b->buf[b->next_buf];
+  const RoundPlan& r = b->rounds[0];
+  BCK(b, cudaMemsetAsync(b->job_uid, 0, J * sizeof(int64_t), b->sst));
+  BCK(b, enqueue_sample(b, rb, r.view, r.max_region, ep));
+  BCK(b, cudaEventRecord(rb.ready, b->sst));
+  b->presampled = true;
+  return FW2V_OK;
+}
+
+// Undo a sampling ahead (before the jobs, the plan or buf[0] change).
+fw2v_status cancel_presample(fw2v_batch* b) {
+  if (!b->presampled) return FW2V_OK;
+  const size_t J = b->jobs.size();
+  const int64_t G = b->n_gstreams;
+  BCK(b, cudaStreamSynchronize(b->sst));
+  BCK(b, cudaMemcpy(b->lcg, b->pre_lcg, G * 8, cudaMemcpyDeviceToDevice));
+  BCK(b, cudaMemcpy(b->wca, b->pre_wca, G * 8, cudaMemcpyDeviceToDevice));
+  BCK(b, cudaMemcpy(b->alpha, b->pre_alpha, G * 4, cudaMemcpyDeviceToDevice));
+  BCK(b, cudaMemcpy(b->job_uid, b->pre_uid, J * 8, cudaMemcpyDeviceToDevice));
+  BCK(b, cudaMemcpy(b->job_words, b->pre_words, J * 8, cudaMemcpyDeviceToDevice));
+  BCK(b, cudaMemcpy(b->job_kept, b->pre_kept, J * 8, cudaMemcpyDeviceToDevice));
+  b->presampled = false;
+  return FW2V_OK;
 }
 
 fw2v_status check_error_flag(fw2v_batch* b, const char* what) {
@@ -604,6 +669,8 @@ void fw2v_batch_destroy(fw2v_batch* b) {
   bfree(b->jump_a); bfree(b->jump_c); bfree(b->exp_table); bfree(b->error_flag); bfree(b->counter);
   bfree(b->lcg); bfree(b->wca); bfree(b->alpha);
   bfree(b->job_uid); bfree(b->job_words); bfree(b->job_kept); bfree(b->orig_scratch);
+  bfree(b->pre_lcg); bfree(b->pre_wca); bfree(b->pre_alpha); bfree(b->pre_uid); bfree(b->pre_words);
+  bfree(b->pre_kept);
   for (RoundBuf& rb : b->buf)
     for (cudaEvent_t e : {rb.ready, rb.freed})
       if (e) cudaEventDestroy(e);
@@ -633,6 +700,8 @@ fw2v_status fw2v_batch_add_job(fw2v_batch* b, const fw2v_config* cfg, const uint
     if (chunk_off[i] < 0 || chunk_off[i] >= stream_len)
       return bfail(b, FW2V_ERR_ARGUMENT, "batch job: chunk %lld starts outside the stream", (long long)i);
   BCK(b, cudaSetDevice(b->cfg.device));
+  fw2v_status pre = cancel_presample(b);
+  if (pre != FW2V_OK) return pre;
   BCK(b, cudaStreamSynchronize(b->st));
   BCK(b, cudaStreamSynchronize(b->sst));
   BatchJob j;
@@ -715,11 +784,15 @@ fw2v_status fw2v_batch_add_job(fw2v_batch* b, const fw2v_config* cfg, const uint
   const int64_t J = (int64_t)b->jobs.size() + 1;
   if (J > b->job_cap) {
     const int64_t cap = std::max<int64_t>(J, b->job_cap * 2);
-    if (grow(b->job_uid, 0, cap) != cudaSuccess || grow(b->job_words, 0, cap) != cudaSuccess ||
-        grow(b->job_kept, 0, cap) != cudaSuccess)
+    const int64_t old = (int64_t)b->jobs.size();
+    if (grow(b->job_uid, 0, cap) != cudaSuccess || grow(b->job_words, old, cap) != cudaSuccess ||
+        grow(b->job_kept, old, cap) != cudaSuccess)
       return undo(bfail(b, FW2V_ERR_NOMEM, "batch job counters"));
     b->job_cap = cap;
   }
+  if (cudaMemset(b->job_words + b->jobs.size(), 0, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMemset(b->job_kept + b->jobs.size(), 0, sizeof(unsigned long long)) != cudaSuccess)
+    return undo(bfail(b, FW2V_ERR_CUDA, "batch job counters"));
   if (b->negative < 0) {
     b->negative = c.negative;
     const int n_jump = 32 * (1 + c.negative) + 1;
@@ -738,6 +811,15 @@ fw2v_status fw2v_batch_add_job(fw2v_batch* b, const fw2v_config* cfg, const uint
   b->jobs.push_back(std::move(j));
   b->words_total.push_back(0);
   b->kept_total.push_back(0);
+  b->words_snap.push_back(0);
+  b->kept_snap.push_back(0);
+  // the undo snapshots are sized by the stream and job counts: reallocated on use
+  bfree(b->pre_lcg);
+  bfree(b->pre_wca);
+  bfree(b->pre_alpha);
+  bfree(b->pre_uid);
+  bfree(b->pre_words);
+  bfree(b->pre_kept);
   b->planned = false;
   if (job_out) *job_out = (int32_t)b->jobs.size() - 1;
   return FW2V_OK;
@@ -809,10 +891,9 @@ fw2v_status fw2v_batch_train_epochs(fw2v_batch* b, int32_t n_epochs, fw2v_batch_
     return FW2V_OK;
   }
   const size_t J = b->jobs.size();
-  BCK(b, cudaMemsetAsync(b->job_words, 0, J * sizeof(unsigned long long), b->st));
-  BCK(b, cudaMemsetAsync(b->job_kept, 0, J * sizeof(unsigned long long), b->st));
   BCK(b, cudaStreamSynchronize(b->st));
   BCK(b, cudaEventRecord(b->ev_start, b->st));
+  if (b->presampled) BCK(b, cudaStreamWaitEvent(b->st, b->buf[b->next_buf].ready, 0));
   if (b->cfg.use_graph) {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -833,20 +914,29 @@ fw2v_status fw2v_batch_train_epochs(fw2v_batch* b, int32_t n_epochs, fw2v_batch_
     BCK(b, cudaEventRecord(b->ev_end, b->st));
     BCK(b, cudaStreamSynchronize(b->st));
   }
+  b->presampled = false;
+  b->next_buf = (int)((b->next_buf + (int64_t)epochs * (int64_t)b->rounds.size()) % 2);
   s = check_error_flag(b, "batch train");
   if (s != FW2V_OK) return s;
+  // the job counters are cumulative: this call's words are the change
   std::vector<unsigned long long> w(J), k(J);
   BCK(b, cudaMemcpy(w.data(), b->job_words, J * 8, cudaMemcpyDeviceToHost));
   BCK(b, cudaMemcpy(k.data(), b->job_kept, J * 8, cudaMemcpyDeviceToHost));
   fw2v_batch_stats out{};
   for (size_t i = 0; i < J; i++) {
-    b->words_total[i] += w[i];
-    b->kept_total[i] += k[i];
-    out.words_read += w[i];
-    out.words_kept += k[i];
+    out.words_read += w[i] - b->words_snap[i];
+    out.words_kept += k[i] - b->kept_snap[i];
+    b->words_total[i] = w[i];
+    b->kept_total[i] = k[i];
   }
+  b->words_snap = w;
+  b->kept_snap = k;
   b->epochs_run += epochs;
   BCK(b, cudaEventElapsedTime(&out.ms, b->ev_start, b->ev_end));
+  if (b->epochs_run < max_epochs) {  // the next call's first round, while the host returns
+    s = presample(b, b->epochs_run);
+    if (s != FW2V_OK) return s;
+  }
   out.epochs = epochs;
   out.rounds = (int32_t)b->rounds.size();
   if (stats) *stats = out;
@@ -930,7 +1020,9 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
   if (!b) return FW2V_ERR_ARGUMENT;
   if (b->cfg.deterministic) return bfail(b, FW2V_ERR_STATE, "tuning needs the concurrent mode");
   BCK(b, cudaSetDevice(b->cfg.device));
-  fw2v_status s = plan(b);
+  fw2v_status s = cancel_presample(b);
+  if (s != FW2V_OK) return s;
+  s = plan(b);
   if (s != FW2V_OK) return s;
   if (sample_tokens <= 0) sample_tokens = (int64_t)1 << 23;
   const size_t J = b->jobs.size();
@@ -1001,6 +1093,9 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
     }
   }
 
+  std::vector<unsigned long long> words0(J), kept0(J);  // tuning samples must not count
+  BCK(b, cudaMemcpy(words0.data(), b->job_words, J * 8, cudaMemcpyDeviceToHost));
+  BCK(b, cudaMemcpy(kept0.data(), b->job_kept, J * 8, cudaMemcpyDeviceToHost));
   fw2v_batch_tune_report rep{};
   rep.n_classes = (int32_t)keys.size();
   auto sample_into_buf0 = [&](const RoundPlan& r) -> fw2v_status {
@@ -1108,6 +1203,9 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
     rep.blocks_per_sm[fam] = b->blocks_per_sm[fam];
   }
   b->planned = false;  // shapes may have moved jobs between families
+  cudaStreamSynchronize(b->sst);
+  cudaMemcpy(b->job_words, words0.data(), J * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(b->job_kept, kept0.data(), J * 8, cudaMemcpyHostToDevice);
   const cudaError_t e = restore();
   if (result != FW2V_OK) return result;
   BCK(b, e);

@@ -229,3 +229,16 @@ def test_batch_rejects_bad_jobs(jobs):
         bad[3] = len(corpus.counts) + 7
         with pytest.raises(fw2v.Fw2vError):
             b.add_job(_config(over), corpus.counts, corpus.train_words, bad, corpus.chunk_off)
+
+
+def test_tuning_between_epochs_undoes_the_sampling_ahead(jobs):
+    """After a call the next epoch's first round is sampled ahead; tuning (or a
+    new plan) undoes it, so the streams continue exactly."""
+    sel = [jobs[0], jobs[2]]  # two and three epochs
+    with _batch(sel, round_tokens=20000) as b:
+        first = b.train_epochs(1)
+        b.tune(sample_tokens=3000)
+        rest = b.train()
+        assert first.words_read + rest.words_read == sum(_words(c, o) for c, o in sel)
+        for j, (c, o) in enumerate(sel):
+            assert b.job_words(j)[0] == _words(c, o)
