@@ -252,9 +252,9 @@ void free_plan(fw2v_batch* b) {
   b->planned = false;
 }
 
-int64_t shape_smem_floats(const BatchJob& j) {
+int64_t shape_smem_floats(const BatchJob& j, int elem) {
   const bool pre = j.prefetch && j.cfg.negative + 1 <= j.stages;
-  return (int64_t)(2 * j.cfg.window + 1 + 3 + (pre ? 2 : 1) * j.stages) * j.pitch;
+  return ((int64_t)(2 * j.cfg.window + 2) * j.pitch * 4 + (int64_t)((pre ? 2 : 1) * j.stages + 2) * j.pitch * elem) / 4;
 }
 int64_t shape_scratch_elems(const BatchJob& j) { return (int64_t)(2 * j.cfg.window + 1) * j.pitch; }
 
@@ -442,7 +442,8 @@ struct Grid {
 fw2v_status grid_for(fw2v_batch* b, const std::vector<int>& active, int fam, int wpb, int cap, Grid* g) {
   g->smem_floats = 0;
   for (int j : active)
-    if (b->jobs[j].family() == fam) g->smem_floats = std::max(g->smem_floats, shape_smem_floats(b->jobs[j]));
+    if (b->jobs[j].family() == fam)
+      g->smem_floats = std::max(g->smem_floats, shape_smem_floats(b->jobs[j], (int)b->elem));
   if (g->smem_floats == 0) return FW2V_OK;
   const int det = b->cfg.deterministic;
   cudaError_t e = cudaErrorInvalidValue;

@@ -15,7 +15,7 @@ extern "C" void fw2v_exp_table(float* t);
 
 namespace fw2v {
 cudaError_t launch_train(const TrainParams& p, int num_sms, cudaStream_t st);
-size_t train_smem_bytes(int window, int64_t pitch, int warps, int r, bool prefetch);
+size_t train_smem_bytes(int window, int64_t pitch, int warps, int r, bool prefetch, int elem);
 int64_t train_scratch_warps(int num_sms);
 }  // namespace fw2v
 

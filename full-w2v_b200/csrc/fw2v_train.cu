@@ -51,10 +51,11 @@ LaunchShape choose_shape(int d, int negative) {
   return s;
 }
 
-// Shared memory of one block: per warp, the ring of 2W+1 rows, a sink row, R
-// target rows (two sets with the prefetch) and two staging rows (WarpRows).
-size_t train_smem_bytes(int window, int64_t pitch, int warps, int r, bool prefetch) {
-  return (size_t)warps * (2 * window + 1 + 3 + (prefetch ? 2 : 1) * r) * pitch * sizeof(float);
+// Shared memory of one block: per warp, the FP32 ring of 2W+1 rows and a sink
+// row, then R target rows (two sets with the prefetch) and two staging rows of
+// the table's element type (WarpRows).
+size_t train_smem_bytes(int window, int64_t pitch, int warps, int r, bool prefetch, int elem) {
+  return (size_t)warps * ((size_t)(2 * window + 2) * pitch * 4 + (size_t)((prefetch ? 2 : 1) * r + 2) * pitch * elem);
 }
 
 // Warps the scratch of a handle must cover: every warp the persistent grid can
@@ -80,7 +81,7 @@ static cudaError_t launch_rt(const TrainParams& p, int r, int num_sms, size_t sm
 cudaError_t launch_train(const TrainParams& p, int num_sms, cudaStream_t st) {
   const LaunchShape s = choose_shape(p.d, p.negative);
   const size_t smem = train_smem_bytes(p.window, p.pitch, p.deterministic ? 1 : kWarpsPerBlock, s.r,
-                                       p.prefetch && p.negative + 1 <= s.r);
+                                       p.prefetch && p.negative + 1 <= s.r, p.bf16 ? 2 : 4);
   if (s.vec == 2) return launch_rt<2, 1>(p, s.r, num_sms, smem, st);
   switch (s.nv) {
     case 1: return launch_rt<4, 1>(p, s.r, num_sms, smem, st);

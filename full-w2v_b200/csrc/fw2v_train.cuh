@@ -560,11 +560,37 @@ __device__ __forceinline__ void lds_staged(Row<VEC, NV>& r, uint32_t row, const 
   else lds_row_bf16(r, row, m);
 }
 
+// A row into a staging row of the table's element type; with bfloat16 tables
+// the values must be bfloat16 already (rows as loaded from a table), so
+// keeping their top 16 bits is exact.
+template <typename T, int VEC, int NV>
+__device__ __forceinline__ void sts_staged(const Row<VEC, NV>& r, uint32_t row, const LaneMap<VEC, NV>& m) {
+  if constexpr (std::is_same_v<T, float>) {
+    sts_row(r, row, m);
+  } else {
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+      if (!m.ok[i]) continue;
+      const uint32_t at = row + (m.off[i] / 4) * 2u;
+      const uint32_t a = __byte_perm(__float_as_uint(r.x[i][0]), __float_as_uint(r.x[i][1]), 0x7632);
+      if constexpr (VEC == 4) {
+        const uint32_t b = __byte_perm(__float_as_uint(r.x[i][2]), __float_as_uint(r.x[i][3]), 0x7632);
+        asm volatile("st.shared.v2.u32 [%0], {%1, %2};" ::"r"(at), "r"(a), "r"(b) : "memory");
+      } else {
+        asm volatile("st.shared.u32 [%0], %1;" ::"r"(at), "r"(a) : "memory");
+      }
+    }
+  }
+}
+
 // Shared-memory rows of one warp, each `P` floats.
 template <int R>
 struct WarpRows {
-  // ring, sink, R target rows (2 x R with the target prefetch), 2 staging rows
-  __host__ __device__ static constexpr int rows(int D, bool prefetch) { return D + 1 + (prefetch ? 2 : 1) * R + 2; }
+  // FP32 ring and sink rows, then staged rows of the table's element type: R
+  // target originals (2 x R with the target prefetch) and 2 staging rows
+  __host__ __device__ static constexpr int64_t bytes(int D, bool prefetch, int64_t pitch, int elem) {
+    return (int64_t)(D + 1) * pitch * 4 + (int64_t)((prefetch ? 2 : 1) * R + 2) * pitch * elem;
+  }
 };
 
 // One sentence on one warp.
@@ -619,6 +645,9 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   const LaneMap<VEC, NV> lm(lane, d);
   const uint32_t ring_b = smem_addr(ring);
   const uint32_t row_bytes = (uint32_t)P * 4u;
+  // staged rows (target originals, entering and leaving copies) hold the
+  // table's element type: half size with bfloat16 tables
+  const uint32_t srow_bytes = (uint32_t)P * (uint32_t)sizeof(T);
   const uint32_t sink_b = ring_b + (uint32_t)D * row_bytes;
   // Target rows.  With the prefetch (all 1 + K targets of a centre in one
   // group), two sets of R rows: centre w's rows were copied (cp.async, table
@@ -626,13 +655,13 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   // the originals for the write-back.  Otherwise one set holds the FP32
   // originals of the current group, loaded when it starts.
   const uint32_t o0_b = sink_b + row_bytes;
-  const uint32_t o1_b = o0_b + (uint32_t)R * row_bytes;
-  const uint32_t in_b = pre ? o1_b + (uint32_t)R * row_bytes : o1_b;
-  const uint32_t out_b = in_b + row_bytes;
+  const uint32_t o1_b = o0_b + (uint32_t)R * srow_bytes;
+  const uint32_t in_b = pre ? o1_b + (uint32_t)R * srow_bytes : o1_b;
+  const uint32_t out_b = in_b + srow_bytes;
   auto prefetch_targets = [&](uint32_t set, int my_target) {
     for (int k = 0; k <= K; k++) {
       const int tk = __shfl_sync(kFull, my_target, k);
-      cp_row(set + (uint32_t)k * row_bytes, syn1neg + (int64_t)tk * P, lm, d);
+      cp_row(set + (uint32_t)k * srow_bytes, syn1neg + (int64_t)tk * P, lm, d);
     }
   };
 
@@ -706,14 +735,14 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
                 bool stale = false;
                 for (int j = 0; j <= K; j++) stale |= __shfl_sync(kFull, t_prev, j) == tk;
                 if (stale) {
-                  cp_row(cur_b + (uint32_t)k * row_bytes, syn1neg + (int64_t)tk * P, lm, d);
+                  cp_row(cur_b + (uint32_t)k * srow_bytes, syn1neg + (int64_t)tk * P, lm, d);
                   cp_async_commit();
                   cp_async_wait();
                 }
-                lds_staged<T>(o[k], cur_b + (uint32_t)k * row_bytes, lm);
+                lds_staged<T>(o[k], cur_b + (uint32_t)k * srow_bytes, lm);
               } else {
                 row_load_global(o[k], syn1neg + (int64_t)tk * P, lane, d);
-                sts_row(o[k], o0_b + (uint32_t)k * row_bytes, lm);
+                sts_staged<T>(o[k], o0_b + (uint32_t)k * srow_bytes, lm);
               }
             } else {
               row_zero(o[k]);
@@ -761,8 +790,7 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
             const int tk = __shfl_sync(kFull, my_t, k);
             if (k < nt) {
               Row<VEC, NV> o0;
-              if (pre) lds_staged<T>(o0, cur_b + (uint32_t)k * row_bytes, lm);
-              else lds_row(o0, o0_b + (uint32_t)k * row_bytes, lm);
+              lds_staged<T>(o0, (pre ? cur_b : o0_b) + (uint32_t)k * srow_bytes, lm);
               row_add_delta(syn1neg + (int64_t)tk * P, o[k], o0, lane, d,
                             sr_event_key(skey, (uint64_t)w * (K + 1) + (k0 + k)),
                             (uint64_t)tk);
@@ -847,7 +875,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MinBlocks<NV>::value) sgn
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int D = 2 * p.window + 1;
-  float* ring = smem + (int64_t)warp * WarpRows<R>::rows(D, p.prefetch && p.negative + 1 <= R) * p.pitch;
+  float* ring = smem + (int64_t)warp *
+                           WarpRows<R>::bytes(D, p.prefetch && p.negative + 1 <= R, p.pitch, (int)sizeof(T)) / 4;
   const int64_t gwarp = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
   T* orig = reinterpret_cast<T*>(p.orig_scratch) + gwarp * D * p.pitch;
   const int64_t total = total_sentences(p);

@@ -167,11 +167,11 @@ def test_jobs_manifest_trains_each_job_as_alone(tmp_path, precision):
     for i, (name, seed) in enumerate((("zipf_t1", 0), ("messy_t1", 9))):
         g = load(name)
         (tmp_path / f"c{i}.txt").write_bytes(g["text"])
-        args = ["-train", f"c{i}.txt", "-output", f"j{i}.vec", "-binary", "1", "-seed", str(seed), "-size",
-                str(16 + 24 * i)] + _flags(g, drop=("-negative", "-size"))
-        lines.append(" ".join(args + ["-negative", "5"]))
-        _run(args + ["-negative", "5", "-output", f"a{i}.vec", "-debug", "0", "-deterministic", "1",
-                     "-precision", precision], tmp_path)
+        common = ["-train", f"c{i}.txt", "-binary", "1", "-seed", str(seed), "-size", str(16 + 24 * i),
+                  "-negative", "5"] + _flags(g, drop=("-negative", "-size"))
+        lines.append(" ".join(common + ["-output", f"j{i}.vec"]))
+        _run(common + ["-output", f"a{i}.vec", "-debug", "0", "-deterministic", "1", "-precision", precision],
+             tmp_path)
     (tmp_path / "jobs.txt").write_text("# two jobs\n" + "\n".join(lines) + "\n")
     out = _run(["-jobs", "jobs.txt", "-deterministic", "1", "-precision", precision], tmp_path)
     assert "Job 2 Words:" in out and "Overall Words Per Second:" in out
