@@ -612,7 +612,7 @@ def synth_text(args, cfg):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fw2v", choices=["fw2v", "reference"])
     ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c4", "c5"])
