@@ -184,6 +184,7 @@ struct fw2v_batch {
   unsigned long long* pre_words = nullptr;
   unsigned long long* pre_kept = nullptr;
   std::vector<unsigned long long> words_snap, kept_snap;  // counters at the end of the last call
+  std::vector<cudaEvent_t> round_ev;  // 2 per training launch of a call: its device time
 };
 
 namespace {
@@ -505,8 +506,9 @@ cudaError_t enqueue_sample(fw2v_batch* b, RoundBuf& rb, const BatchRound& r, int
 // Every round of epochs [e0, e0 + epochs): sampler stream and training stream
 // joined by events, ending with the sampler stream joined into the training
 // stream.  Jobs past their own epoch count sample nothing in an epoch.
-cudaError_t enqueue_epochs(fw2v_batch* b, int e0, int epochs, const Grid* grids) {
+cudaError_t enqueue_epochs(fw2v_batch* b, int e0, int epochs, const Grid* grids, bool graph) {
   cudaError_t e = cudaEventRecord(b->ev_fork, b->st);
+  const unsigned ev_flags = graph ? cudaEventRecordExternal : cudaEventRecordDefault;
   if (e == cudaSuccess) e = cudaStreamWaitEvent(b->sst, b->ev_fork, 0);
   int64_t k = 0;
   for (int ep = e0; ep < e0 + epochs && e == cudaSuccess; ep++) {
@@ -525,7 +527,9 @@ cudaError_t enqueue_epochs(fw2v_batch* b, int e0, int epochs, const Grid* grids)
       }
       if (e == cudaSuccess) e = cudaMemsetAsync(b->counter, 0, sizeof(unsigned long long), b->st);
       const Grid& g = grids[r.family];
+      if (e == cudaSuccess) e = cudaEventRecordWithFlags(b->round_ev[2 * k], b->st, ev_flags);
       if (e == cudaSuccess) e = launch_train_round(b, r.family, train_args(b, rb, r.view, ep, g), g, b->st);
+      if (e == cudaSuccess) e = cudaEventRecordWithFlags(b->round_ev[2 * k + 1], b->st, ev_flags);
       if (e == cudaSuccess) e = cudaEventRecord(rb.freed, b->st);
     }
   }
@@ -677,6 +681,7 @@ void fw2v_batch_destroy(fw2v_batch* b) {
       if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : {b->ev_start, b->ev_end, b->ev_fork, b->ev_join})
     if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : b->round_ev) cudaEventDestroy(e);
   if (b->st) cudaStreamDestroy(b->st);
   if (b->sst) cudaStreamDestroy(b->sst);
   delete b;
@@ -892,6 +897,12 @@ fw2v_status fw2v_batch_train_epochs(fw2v_batch* b, int32_t n_epochs, fw2v_batch_
     return FW2V_OK;
   }
   const size_t J = b->jobs.size();
+  const size_t launches = (size_t)epochs * b->rounds.size();
+  while (b->round_ev.size() < 2 * launches) {
+    cudaEvent_t ev;
+    BCK(b, cudaEventCreate(&ev));
+    b->round_ev.push_back(ev);
+  }
   BCK(b, cudaStreamSynchronize(b->st));
   BCK(b, cudaEventRecord(b->ev_start, b->st));
   if (b->presampled) BCK(b, cudaStreamWaitEvent(b->st, b->buf[b->next_buf].ready, 0));
@@ -899,7 +910,7 @@ fw2v_status fw2v_batch_train_epochs(fw2v_batch* b, int32_t n_epochs, fw2v_batch_
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     BCK(b, cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
-    const cudaError_t e = enqueue_epochs(b, e0, epochs, g);
+    const cudaError_t e = enqueue_epochs(b, e0, epochs, g, true);
     const cudaError_t e2 = cudaStreamEndCapture(b->st, &graph);
     BCK(b, e);
     BCK(b, e2);
@@ -911,7 +922,7 @@ fw2v_status fw2v_batch_train_epochs(fw2v_batch* b, int32_t n_epochs, fw2v_batch_
     cudaGraphDestroy(graph);
     BCK(b, e3);
   } else {
-    BCK(b, enqueue_epochs(b, e0, epochs, g));
+    BCK(b, enqueue_epochs(b, e0, epochs, g, false));
     BCK(b, cudaEventRecord(b->ev_end, b->st));
     BCK(b, cudaStreamSynchronize(b->st));
   }
@@ -934,6 +945,16 @@ fw2v_status fw2v_batch_train_epochs(fw2v_batch* b, int32_t n_epochs, fw2v_batch_
   b->kept_snap = k;
   b->epochs_run += epochs;
   BCK(b, cudaEventElapsedTime(&out.ms, b->ev_start, b->ev_end));
+  for (size_t i = 0; i < launches; i++) {
+    float t = 0;
+    if (cudaEventElapsedTime(&t, b->round_ev[2 * i], b->round_ev[2 * i + 1]) != cudaSuccess) {
+      cudaGetLastError();
+      out.train_ms = -1.0f;  // not timed
+      break;
+    }
+    out.train_ms += t;
+  }
+  out.train_launches = (int32_t)launches;
   if (b->epochs_run < max_epochs) {  // the next call's first round, while the host returns
     s = presample(b, b->epochs_run);
     if (s != FW2V_OK) return s;

@@ -55,7 +55,8 @@ class BatchConfig(C.Structure):
 
 class BatchStats(C.Structure):
     _fields_ = [("words_read", C.c_uint64), ("words_kept", C.c_uint64), ("ms", C.c_float),
-                ("epochs", C.c_int32), ("rounds", C.c_int32)]
+                ("epochs", C.c_int32), ("rounds", C.c_int32), ("train_ms", C.c_float),
+                ("train_launches", C.c_int32)]
 
 
 class TuneReport(C.Structure):

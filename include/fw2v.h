@@ -266,8 +266,10 @@ typedef struct fw2v_batch_stats {
   uint64_t words_read;    /* tokens read by all jobs' streams in the call */
   uint64_t words_kept;
   float ms;               /* device time of the call (sampling and training) */
-  int32_t epochs;         /* epochs run: the largest job epoch count */
+  int32_t epochs;         /* epochs run in the call */
   int32_t rounds;         /* rounds per epoch */
+  float train_ms;         /* device time of the training kernel launches, summed (-1: not timed) */
+  int32_t train_launches; /* training kernel launches in the call */
 } fw2v_batch_stats;
 
 void fw2v_batch_config_default(fw2v_batch_config* cfg);
