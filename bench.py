@@ -272,7 +272,14 @@ def run_own(args, world, rank, local):
             b = fw2v.Batch(precision=prec, device=local)
             b.add_job(job_config(args, cfg, T, epochs, prec), corpus.counts, corpus.train_words, corpus.stream,
                       corpus.chunk_off)
-            tuned = b.tune(cache=tune_cache)
+            if args.shape:  # a given shape instead of the tuner's
+                b.set_shape(0, *[int(x) for x in args.shape.split(",")])
+                if args.wpb:
+                    for f in range(3):
+                        b.set_launch(f, min(args.wpb, 8 if f == 0 else 4))
+                tuned = {"given": args.shape, "warps_per_block": args.wpb}
+            else:
+                tuned = b.tune(cache=tune_cache)
 
             def run_epoch():
                 # per round: sampler, negatives, entry prefix, job bookkeeping, trainer
@@ -328,7 +335,13 @@ def run_own(args, world, rank, local):
             with fw2v.Batch(precision=prec, device=local) as eb:
                 eb.add_job(job_config(args, cfg, T, 1, prec), corpus.counts, corpus.train_words, host_stream,
                            corpus.chunk_off)
-                eb.tune(cache=tune_cache)  # the shapes chosen above, from the cache
+                if args.shape:
+                    eb.set_shape(0, *[int(x) for x in args.shape.split(",")])
+                    if args.wpb:
+                        for f in range(3):
+                            eb.set_launch(f, min(args.wpb, 8 if f == 0 else 4))
+                else:
+                    eb.tune(cache=tune_cache)  # the shapes chosen above, from the cache
                 st = eb.train_epochs(1)
                 e2e_words += st.words_read
         else:
@@ -645,6 +658,8 @@ def main():
                          "single-job kernel")
     ap.add_argument("--heldout", type=int, default=1_000_000, help="held-out tokens (c3)")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP32 comparison run")
+    ap.add_argument("--shape", default=None, help="batched forms: lane_vec,lane_nv,stages,prefetch instead of tuning")
+    ap.add_argument("--wpb", type=int, default=0, help="batched forms with --shape: warps per block")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     world, rank, local = dist_setup()
