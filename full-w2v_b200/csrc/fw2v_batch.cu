@@ -72,7 +72,7 @@ struct BatchJob {
   std::vector<int64_t> sbase;  // threads + 1: readable-token prefix of its streams
   int64_t gfirst = 0;          // global number of its stream 0
   int lane_vec = 4, lane_nv = 1, stages = 6;
-  int prefetch = 0;  // target rows copied one centre ahead (one group of targets only)
+  int prefetch = 0;  // target rows of each group copied while the previous group trains
   int family() const { return batch_family(lane_nv, stages); }
 };
 
@@ -254,7 +254,7 @@ void free_plan(fw2v_batch* b) {
 }
 
 int64_t shape_smem_floats(const BatchJob& j, int elem) {
-  const bool pre = j.prefetch && j.cfg.negative + 1 <= j.stages;
+  const bool pre = j.prefetch != 0;
   return ((int64_t)(2 * j.cfg.window + 2) * j.pitch * 4 + (int64_t)((pre ? 2 : 1) * j.stages + 2) * j.pitch * elem) / 4;
 }
 int64_t shape_scratch_elems(const BatchJob& j) { return (int64_t)(2 * j.cfg.window + 1) * j.pitch; }
@@ -1153,7 +1153,6 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
       for (int st : kBatchStages) {
         for (int pre : {0, 1}) {
           if (result != FW2V_OK || !valid_shape(d_max, vec, def_nv, st)) continue;
-          if (pre && b->negative + 1 > st) continue;  // the prefetch needs all targets in one group
           for (int j : members[c]) {
             b->jobs[j].lane_vec = vec;
             b->jobs[j].lane_nv = def_nv;

@@ -81,7 +81,7 @@ static cudaError_t launch_rt(const TrainParams& p, int r, int num_sms, size_t sm
 cudaError_t launch_train(const TrainParams& p, int num_sms, cudaStream_t st) {
   const LaunchShape s = choose_shape(p.d, p.negative);
   const size_t smem = train_smem_bytes(p.window, p.pitch, p.deterministic ? 1 : kWarpsPerBlock, s.r,
-                                       p.prefetch && p.negative + 1 <= s.r, p.bf16 ? 2 : 4);
+                                       p.prefetch != 0, p.bf16 ? 2 : 4);
   if (s.vec == 2) return launch_rt<2, 1>(p, s.r, num_sms, smem, st);
   switch (s.nv) {
     case 1: return launch_rt<4, 1>(p, s.r, num_sms, smem, st);

@@ -143,6 +143,8 @@ __device__ __forceinline__ void cp_row(uint32_t dst, const float* src, const Lan
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// All but the most recently committed group complete.
+__device__ __forceinline__ void cp_async_wait_but_last() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 template <int VEC, int NV>
 __device__ __forceinline__ void row_zero(Row<VEC, NV>& r) {
@@ -616,7 +618,7 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   T* const syn1neg = reinterpret_cast<T*>(p.syn1neg);
   const float alpha = sn.alpha;
   const bool one_group = K + 1 <= R;
-  const bool pre = one_group && p.prefetch;  // target rows copied one centre ahead
+  const bool pre = p.prefetch != 0;  // target rows copied one group of targets ahead
   const uint64_t skey = sr_sentence_key(p.sr_seed, (uint64_t)sn.uid);  // bfloat16 tables only
 
   // Every id is checked before any table access.
@@ -649,17 +651,18 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   // table's element type: half size with bfloat16 tables
   const uint32_t srow_bytes = (uint32_t)P * (uint32_t)sizeof(T);
   const uint32_t sink_b = ring_b + (uint32_t)D * row_bytes;
-  // Target rows.  With the prefetch (all 1 + K targets of a centre in one
-  // group), two sets of R rows: centre w's rows were copied (cp.async, table
-  // element type) into set w % 2 while centre w-1 trained, and stay there as
-  // the originals for the write-back.  Otherwise one set holds the FP32
-  // originals of the current group, loaded when it starts.
+  // Target rows, in the table's element type.  With the prefetch, two sets of
+  // R rows: the rows of each group of targets (R of a centre's 1 + K, in
+  // centre order) are copied (cp.async, each lane its own elements) into one
+  // set while the previous group trains, and stay there as the originals for
+  // the write-back.  Otherwise one set holds the originals of the current
+  // group, loaded when it starts.
   const uint32_t o0_b = sink_b + row_bytes;
   const uint32_t o1_b = o0_b + (uint32_t)R * srow_bytes;
   const uint32_t in_b = pre ? o1_b + (uint32_t)R * srow_bytes : o1_b;
   const uint32_t out_b = in_b + srow_bytes;
-  auto prefetch_targets = [&](uint32_t set, int my_target) {
-    for (int k = 0; k <= K; k++) {
+  auto prefetch_targets = [&](uint32_t set, int my_target, int n) {
+    for (int k = 0; k < n; k++) {
       const int tk = __shfl_sync(kFull, my_target, k);
       cp_row(set + (uint32_t)k * srow_bytes, syn1neg + (int64_t)tk * P, lm, d);
     }
@@ -677,23 +680,23 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   }
 
   int t_next = one_group ? target_id(ids, negs, K, 0, 0, K + 1, lane) : 0;
+  // cp.async commit groups with the prefetch: the first group's rows before
+  // the loop, then at every centre its staging copies (Enter) and at every
+  // group of targets the next group's rows.
+  const int nt0 = K + 1 < R ? K + 1 : R;
+  uint32_t cur_b = o0_b;  // the set holding the rows of the group about to train
   if (pre) {
-    prefetch_targets(o0_b, t_next);
+    if (L >= 2) prefetch_targets(o0_b, target_id(ids, negs, K, 0, 0, nt0, lane), nt0);
     cp_async_commit();
-    cp_async_wait();
   }
-  int t_prev = -1;  // lane k: target k of the previous centre if it wrote it back
+  int t_prev = -1;  // lane k < R: target k of the previous group of targets (written back), else -1
   for (int w = 0; w < L; w++) {
     // Ids and rows needed later in this centre, loaded ahead of use.
     const int q_out = w - W, q_in = w + W + 1;
     const int id_out = q_out >= 0 ? __ldg(ids + q_out) : -1;
     const int id_in = q_in < L ? __ldg(ids + q_in) : -1;
     const int t_here = t_next;
-    const uint32_t cur_b = (w & 1) ? o1_b : o0_b;
-    if (one_group && w + 1 < L) {
-      t_next = target_id(ids, negs, K, w + 1, 0, K + 1, lane);
-      if (pre) prefetch_targets((w & 1) ? o0_b : o1_b, t_next);
-    }
+    if (one_group && w + 1 < L) t_next = target_id(ids, negs, K, w + 1, 0, K + 1, lane);
     // The entering row can be fetched now unless the leaving position holds
     // the same word (its write-back must land first).  Both staging copies run
     // in the background while the centre trains.
@@ -713,10 +716,42 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
     const unsigned mask = __ballot_sync(kFull, valid);
     const int nctx = __popc(mask);
 
+    int prefetches = 0;  // groups committed after this centre's staging copies
     if (nctx > 0) {
       for (int k0 = 0; k0 <= K; k0 += R) {
         const int nt = (K + 1 - k0) < R ? (K + 1 - k0) : R;
         const int my_t = one_group ? t_here : target_id(ids, negs, K, w, k0, nt, lane);
+        if (pre) {
+          // This group's rows: committed before this centre's staging copies
+          // for its first group, before the previous group's prefetch otherwise.
+          if (k0 == 0) cp_async_wait_but_last();
+          else cp_async_wait();
+          // A row copied before the previous group's write-back of the same
+          // target is fetched again (after this lane's own reduction, in
+          // program order).
+          bool stale_any = false;
+          for (int k = 0; k < nt; k++) {
+            const int tk = __shfl_sync(kFull, my_t, k);
+            bool stale = false;
+            for (int j = 0; j < R; j++) stale |= __shfl_sync(kFull, t_prev, j) == tk;
+            if (stale) cp_row(cur_b + (uint32_t)k * srow_bytes, syn1neg + (int64_t)tk * P, lm, d);
+            stale_any |= stale;
+          }
+          if (stale_any) {
+            cp_async_commit();
+            cp_async_wait();
+          }
+          // the next group's rows, into the other set
+          const uint32_t nxt_b = cur_b == o0_b ? o1_b : o0_b;
+          if (k0 + R <= K) {
+            const int nt1 = (K + 1 - k0 - R) < R ? (K + 1 - k0 - R) : R;
+            prefetch_targets(nxt_b, target_id(ids, negs, K, w, k0 + R, nt1, lane), nt1);
+          } else if (w + 1 < L) {
+            prefetch_targets(nxt_b, target_id(ids, negs, K, w + 1, 0, nt0, lane), nt0);
+          }
+          cp_async_commit();
+          prefetches++;
+        }
         bool dup = false;
         for (int j = 0; j + 1 < nt; j++) {
           const int tj = __shfl_sync(kFull, my_t, j);
@@ -729,16 +764,6 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
             const int tk = __shfl_sync(kFull, my_t, k);
             if (k < nt) {
               if (pre) {
-                // The copy was taken before the previous centre's write-back:
-                // a target it also wrote is fetched again (after this lane's
-                // own reduction, in program order).
-                bool stale = false;
-                for (int j = 0; j <= K; j++) stale |= __shfl_sync(kFull, t_prev, j) == tk;
-                if (stale) {
-                  cp_row(cur_b + (uint32_t)k * srow_bytes, syn1neg + (int64_t)tk * P, lm, d);
-                  cp_async_commit();
-                  cp_async_wait();
-                }
                 lds_staged<T>(o[k], cur_b + (uint32_t)k * srow_bytes, lm);
               } else {
                 row_load_global(o[k], syn1neg + (int64_t)tk * P, lane, d);
@@ -819,13 +844,15 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
                           (uint64_t)tk);
           }
         }
+        t_prev = lane < nt ? my_t : -1;
+        if (pre) cur_b = cur_b == o0_b ? o1_b : o0_b;
       }
     }
 
-    t_prev = nctx > 0 ? t_here : -1;
-
     // Slide the window: position w-W leaves, position w+W+1 takes its slot.
-    cp_async_wait();
+    // The staging copies must be complete; the next group's prefetch may run on.
+    if (prefetches > 0) cp_async_wait_but_last();
+    else cp_async_wait();
     if (q_out >= 0) {
       Row<VEC, NV> cur, org;
       lds_row(cur, ring_b + (uint32_t)(q_out % D) * row_bytes, lm);
@@ -876,7 +903,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MinBlocks<NV>::value) sgn
   const int warp = threadIdx.x >> 5;
   const int D = 2 * p.window + 1;
   float* ring = smem + (int64_t)warp *
-                           WarpRows<R>::bytes(D, p.prefetch && p.negative + 1 <= R, p.pitch, (int)sizeof(T)) / 4;
+                           WarpRows<R>::bytes(D, p.prefetch != 0, p.pitch, (int)sizeof(T)) / 4;
   const int64_t gwarp = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
   T* orig = reinterpret_cast<T*>(p.orig_scratch) + gwarp * D * p.pitch;
   const int64_t total = total_sentences(p);

@@ -129,7 +129,8 @@ def test_deterministic_batch_equals_each_job_alone_bf16(jobs):
 
 SHAPES = ([(2, (2, 1, s, 0)) for s in (2, 3, 4, 6)] + [(2, (4, 1, s, 0)) for s in (2, 3, 4, 6)] +
           [(5, (4, 2, s, 0)) for s in (2, 3, 4, 6)] + [(6, (4, 3, s, 0)) for s in (2, 3, 4)] +
-          [(2, (2, 1, 6, 1)), (2, (4, 1, 6, 1)), (5, (4, 2, 6, 1)), (3, (4, 1, 6, 1))])
+          [(2, (2, 1, 6, 1)), (2, (4, 1, 6, 1)), (5, (4, 2, 6, 1)), (3, (4, 1, 6, 1)),
+           (2, (2, 1, 2, 1)), (2, (4, 1, 3, 1)), (5, (4, 2, 3, 1)), (6, (4, 3, 2, 1)), (6, (4, 3, 4, 1))])
 
 
 @pytest.mark.parametrize("job,shape", SHAPES)
