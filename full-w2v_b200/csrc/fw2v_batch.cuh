@@ -45,10 +45,10 @@ constexpr int kBatchStages[] = {2, 3, 4, 6};
 // its bodies sets it for all):
 //   0  rows of one vector per lane (d <= 128: 2-float lanes for d <= 64,
 //      4-float for d <= 128), up to 8 warps per block, 128 registers
-//   1  wide rows (2 or 3 four-float vectors per lane), 2 or 3 stages; 4 warps
-//      per block, 3 blocks per SM
-//   2  wide rows, 4 or 6 stages (4 with 3 vectors); 4 warps per block, 255
-//      registers
+//   1  wide rows: 2 four-float vectors per lane with 2 or 3 stages, 3 vectors
+//      with 2; 4 warps per block, 3 blocks per SM
+//   2  other wide rows (2 vectors: 4 or 6 stages; 3 vectors: 3 or 4); 4 warps
+//      per block, 255 registers
 constexpr int kBatchMaxWarps = 8;
 constexpr int kBatchFamilies = 3;
 template <int FAMILY>
@@ -68,7 +68,7 @@ struct BatchFamily<2> {
 
 // The family of a (lane vector width, vectors per lane, stages) shape.
 __host__ __device__ constexpr int batch_family(int nv, int stages) {
-  return nv == 1 ? 0 : stages <= 3 ? 1 : 2;
+  return nv == 1 ? 0 : (stages == 2 || (nv == 2 && stages == 3)) ? 1 : 2;
 }
 
 // Rows of three vectors per lane stop at 4 stages: their 6-stage body does not
@@ -94,15 +94,15 @@ __device__ __forceinline__ void batch_dispatch(const TrainParams& p, const Sente
     else batch_stages<T, 4, 1>(p, sn, ring, orig, table, lane);
   } else if constexpr (FAMILY == 1) {
     if (p.lane_nv == 3) {
-      if (p.stages == 2) train_sentence<T, 4, 3, 2, 0>(p, sn, ring, orig, table, lane);
-      else train_sentence<T, 4, 3, 3, 0>(p, sn, ring, orig, table, lane);
+      train_sentence<T, 4, 3, 2, 0>(p, sn, ring, orig, table, lane);
     } else {
       if (p.stages == 2) train_sentence<T, 4, 2, 2, 0>(p, sn, ring, orig, table, lane);
       else train_sentence<T, 4, 2, 3, 0>(p, sn, ring, orig, table, lane);
     }
   } else {
     if (p.lane_nv == 3) {
-      train_sentence<T, 4, 3, 4, 0>(p, sn, ring, orig, table, lane);
+      if (p.stages == 3) train_sentence<T, 4, 3, 3, 0>(p, sn, ring, orig, table, lane);
+      else train_sentence<T, 4, 3, 4, 0>(p, sn, ring, orig, table, lane);
     } else {
       if (p.stages == 4) train_sentence<T, 4, 2, 4, 0>(p, sn, ring, orig, table, lane);
       else train_sentence<T, 4, 2, 6, 0>(p, sn, ring, orig, table, lane);
