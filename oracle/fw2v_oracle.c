@@ -392,7 +392,8 @@ static uint64_t sr_event_key(uint64_t skey, uint64_t event) {
 }
 static uint64_t sr_vector_bits(uint64_t key, uint64_t row, uint64_t vec) {
   uint32_t lo = fmix32((uint32_t)key ^ ((uint32_t)row * 0x27D4EB2Fu) ^ ((uint32_t)vec * 0x165667B1u));
-  uint32_t hi = fmix32(lo ^ (uint32_t)(key >> 32));
+  uint32_t hi = (lo ^ (uint32_t)(key >> 32)) * 0x9E3779B9u;
+  hi ^= hi >> 15;
   return ((uint64_t)hi << 32) | lo;
 }
 static float bf16_f(uint16_t h) {
