@@ -269,7 +269,7 @@ def run_own(args, world, rank, local):
 
     with ClockSampler(local) as clk:
         if form.endswith("batched"):
-            b = fw2v.Batch(precision=prec, device=local)
+            b = fw2v.Batch(precision=prec, device=local, group_bytes=args.group_bytes)
             b.add_job(job_config(args, cfg, T, epochs, prec), corpus.counts, corpus.train_words, corpus.stream,
                       corpus.chunk_off)
             if args.shape:  # a given shape instead of the tuner's
@@ -332,7 +332,7 @@ def run_own(args, world, rank, local):
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         if form.endswith("batched"):
-            with fw2v.Batch(precision=prec, device=local) as eb:
+            with fw2v.Batch(precision=prec, device=local, group_bytes=args.group_bytes) as eb:
                 eb.add_job(job_config(args, cfg, T, 1, prec), corpus.counts, corpus.train_words, host_stream,
                            corpus.chunk_off)
                 if args.shape:
@@ -470,7 +470,7 @@ def run_c5(args, world, rank, local):
     tokens = [s["nodes"] * s["walks_per_node"] * (s["walk_len"] + 1) for s in all_specs]
     specs = [all_specs[j] for j in assign_jobs(tokens, world)[rank]]
     prec = fw2v.BF16 if args.form.startswith("bf16") else fw2v.FP32
-    batch = fw2v.Batch(precision=prec, device=local)
+    batch = fw2v.Batch(precision=prec, device=local, group_bytes=args.group_bytes)
     labels, alone_p10, alone_ms, alone_words = [], [], 0.0, 0
     for j, s in enumerate(specs):
         corpus, _ = synth.sbm_corpus_gpu(s["nodes"], s["blocks"], s["degree"], s["p_ratio"], s["walks_per_node"],
@@ -516,7 +516,7 @@ def run_c5(args, world, rank, local):
                                   f"rank; form {args.form}", "form": args.form, "jobs": len(all_specs),
                       "jobs_this_rank": len(specs), "scale": args.scale,
                       "parallelism": f"jobs partitioned over {world} ranks" if world > 1 else "single GPU",
-                      "rounds": st.rounds, "tuning": tuned},
+                      "rounds": st.rounds, "group_bytes": args.group_bytes, "tuning": tuned},
            "precision_at_10": {"mean": float(np.nanmean(p10)), "min": float(np.nanmin(p10))},
            "gpu_launches": 5 * st.rounds}
     if alone_p10:
@@ -660,6 +660,8 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP32 comparison run")
     ap.add_argument("--shape", default=None, help="batched forms: lane_vec,lane_nv,stages,prefetch instead of tuning")
     ap.add_argument("--wpb", type=int, default=0, help="batched forms with --shape: warps per block")
+    ap.add_argument("--group-bytes", type=int, default=0,
+                    help="batched forms: table bytes per group of interleaved jobs (0: half of L2, -1: one group)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     world, rank, local = dist_setup()

@@ -8,8 +8,10 @@
 // chunk table.  Sampling streams of all jobs are numbered globally (job j's
 // stream s is gfirst[j] + s) for their carried LCG / word-count / learning-rate
 // state.  An epoch is a fixed sequence of rounds; round r is a list of
-// (job, stream) pairs in the order s = 0, 1, ... and within each s by job, cut
-// where the round's readable tokens would pass round_tokens.  Two sets of
+// (job, stream) pairs in training order (stream_order: groups of jobs whose
+// tables fit the group budget, each group's streams s = 0, 1, ... and within
+// each s by job), cut where the round's readable tokens would pass
+// round_tokens.  Two sets of
 // round buffers (kept ids, their LCG states and negatives, entries) alternate:
 // round r+1 is sampled on the sampler stream while round r trains.
 #include <algorithm>
@@ -74,6 +76,11 @@ struct BatchJob {
   int lane_vec = 4, lane_nv = 1, stages = 6;
   int prefetch = 0;  // target rows of each group copied while the previous group trains
   int family() const { return batch_family(lane_nv, stages); }
+};
+
+struct StreamItem {
+  int32_t job, local;
+  int64_t gstream, tokens;
 };
 
 struct RoundPlan {
@@ -141,6 +148,7 @@ int default_stages(int negative, int nv = 1) {
 struct fw2v_batch {
   fw2v_batch_config cfg{};
   int num_sms = 0;
+  int64_t l2_bytes = 0;
   size_t elem = 4;
   cudaStream_t st = nullptr, sst = nullptr;
   cudaEvent_t ev_start = nullptr, ev_end = nullptr, ev_fork = nullptr, ev_join = nullptr;
@@ -325,6 +333,42 @@ TrainParams train_params(const fw2v_batch* b, const BatchJob& j, const RoundBuf&
 
 fw2v_status cancel_presample(fw2v_batch* b);
 
+// Streams of the jobs with in[j] set, in training order.  Jobs, in index
+// order, are gathered into groups whose tables together fit the group budget
+// (a larger job is a group of its own); a group's streams are taken
+// s = 0, 1, ... and within each s by job.  The work queue hands out sentences
+// in this order, so the warps in flight at any time train a few streams of
+// one group: interleaving its jobs keeps fewer warps at once on any one job's
+// rows than training it alone would, and bounding the group keeps the rows in
+// use resident in L2 between the sentences that touch them.  Each job's own
+// streams keep their order, so deterministic results do not depend on it.
+std::vector<StreamItem> stream_order(const fw2v_batch* b, const std::vector<char>& in) {
+  const int64_t budget = b->cfg.group_bytes ? b->cfg.group_bytes : b->l2_bytes / 2;
+  std::vector<StreamItem> out;
+  size_t g0 = 0;
+  while (g0 < b->jobs.size()) {
+    size_t g1 = g0;
+    int64_t bytes = 0;
+    int max_t = 0;
+    for (; g1 < b->jobs.size(); g1++) {
+      const BatchJob& j = b->jobs[g1];
+      if (!in[g1]) continue;
+      const int64_t tb = 2 * j.V * j.pitch * (int64_t)b->elem;
+      if (budget > 0 && max_t > 0 && bytes + tb > budget) break;
+      bytes += tb;
+      max_t = std::max(max_t, j.cfg.threads);
+    }
+    for (int s = 0; s < max_t; s++)
+      for (size_t ji = g0; ji < g1; ji++) {
+        const BatchJob& j = b->jobs[ji];
+        if (in[ji] && s < j.cfg.threads)
+          out.push_back({(int32_t)ji, s, j.gfirst + s, j.sbase[s + 1] - j.sbase[s]});
+      }
+    g0 = g1;
+  }
+  return out;
+}
+
 // The round plan of an epoch and buffers for its largest round.
 fw2v_status plan(fw2v_batch* b) {
   if (b->planned) return FW2V_OK;
@@ -332,22 +376,11 @@ fw2v_status plan(fw2v_batch* b) {
   const fw2v_status pre = cancel_presample(b);  // its round and buffer are about to go
   if (pre != FW2V_OK) return pre;
   free_plan(b);
-  struct Item {
-    int32_t job, local;
-    int64_t gstream, tokens;
-  };
   const int64_t cap = b->cfg.round_tokens > 0 ? b->cfg.round_tokens : (int64_t)1 << 27;
   for (int fam = 0; fam < kBatchFamilies; fam++) {
-  std::vector<Item> order;
-  int max_t = 0;
-  for (const BatchJob& j : b->jobs)
-    if (j.family() == fam) max_t = std::max(max_t, j.cfg.threads);
-  for (int s = 0; s < max_t; s++)
-    for (size_t ji = 0; ji < b->jobs.size(); ji++) {
-      const BatchJob& j = b->jobs[ji];
-      if (j.family() == fam && s < j.cfg.threads)
-        order.push_back({(int32_t)ji, s, j.gfirst + s, j.sbase[s + 1] - j.sbase[s]});
-    }
+  std::vector<char> in(b->jobs.size());
+  for (size_t ji = 0; ji < b->jobs.size(); ji++) in[ji] = b->jobs[ji].family() == fam;
+  const std::vector<StreamItem> order = stream_order(b, in);
   size_t i = 0;
   while (i < order.size()) {
     size_t e = i;
@@ -359,7 +392,7 @@ fw2v_status plan(fw2v_batch* b) {
     std::vector<int32_t> job(r.n), local(r.n);
     std::vector<int64_t> gs(r.n), kb(r.n + 1, 0);
     for (int g = 0; g < r.n; g++) {
-      const Item& it = order[i + g];
+      const StreamItem& it = order[i + g];
       job[g] = it.job;
       local[g] = it.local;
       gs[g] = it.gstream;
@@ -636,6 +669,7 @@ fw2v_status fw2v_batch_create(const fw2v_batch_config* cfg, fw2v_batch** out) {
   b->cfg = *cfg;
   b->elem = cfg->precision == FW2V_BF16 ? 2 : 4;
   b->num_sms = prop.multiProcessorCount;
+  b->l2_bytes = prop.l2CacheSize;
   auto bad = [&](fw2v_status s) {
     fw2v_batch_destroy(b);
     return s;
@@ -974,29 +1008,23 @@ fw2v_status fw2v_batch_train(fw2v_batch* b, fw2v_batch_stats* stats) {
 // ---- autotuner ----
 namespace {
 
-// A round of the first epoch's (job, stream) order restricted to `jobs`, up to
+// A round of the first epoch's training order restricted to `jobs`, up to
 // `tokens` readable tokens (at least one stream), within the buffer capacity.
 fw2v_status tuning_round(fw2v_batch* b, const std::vector<int>& jobs, int64_t tokens, RoundPlan* r) {
   std::vector<char> in(b->jobs.size(), 0);
   for (int j : jobs) in[j] = 1;
-  int max_t = 0;
-  for (int j : jobs) max_t = std::max(max_t, b->jobs[j].cfg.threads);
   std::vector<int32_t> job, local;
   std::vector<int64_t> gs, kb(1, 0);
-  for (int s = 0; s < max_t; s++)
-    for (size_t ji = 0; ji < b->jobs.size(); ji++) {
-      const BatchJob& j = b->jobs[ji];
-      if (!in[ji] || s >= j.cfg.threads) continue;
-      const int64_t t = j.sbase[s + 1] - j.sbase[s];
-      if (!job.empty() && (kb.back() + t > std::min(tokens, b->buf_kept_cap) ||
-                           (int64_t)job.size() >= b->buf_stream_cap))
-        continue;
-      job.push_back((int32_t)ji);
-      local.push_back(s);
-      gs.push_back(j.gfirst + s);
-      kb.push_back(kb.back() + t);
-      r->max_region = std::max(r->max_region, t);
-    }
+  for (const StreamItem& it : stream_order(b, in)) {
+    if (!job.empty() && (kb.back() + it.tokens > std::min(tokens, b->buf_kept_cap) ||
+                         (int64_t)job.size() >= b->buf_stream_cap))
+      continue;
+    job.push_back(it.job);
+    local.push_back(it.local);
+    gs.push_back(it.gstream);
+    kb.push_back(kb.back() + it.tokens);
+    r->max_region = std::max(r->max_region, it.tokens);
+  }
   r->n = (int)job.size();
   r->kept = kb.back();
   if (r->n == 0 || r->kept > b->buf_kept_cap) return bfail(b, FW2V_ERR_STATE, "tuning sample does not fit");

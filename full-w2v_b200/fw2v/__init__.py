@@ -50,7 +50,8 @@ class EpochStats(C.Structure):
 
 class BatchConfig(C.Structure):
     _fields_ = [("precision", C.c_int32), ("device", C.c_int32), ("use_graph", C.c_int32),
-                ("deterministic", C.c_int32), ("round_tokens", C.c_int64)]
+                ("deterministic", C.c_int32), ("round_tokens", C.c_int64),
+                ("group_bytes", C.c_int64)]
 
 
 class BatchStats(C.Structure):
@@ -350,11 +351,12 @@ class Batch:
     table sigmoid and the same `negative`."""
 
     def __init__(self, precision: int = FP32, device: int = 0, use_graph: bool = True,
-                 deterministic: bool = False, round_tokens: int = 0):
+                 deterministic: bool = False, round_tokens: int = 0, group_bytes: int = 0):
         cfg = BatchConfig()
         lib().fw2v_batch_config_default(C.byref(cfg))
         cfg.precision, cfg.device = precision, device
         cfg.use_graph, cfg.deterministic, cfg.round_tokens = int(use_graph), int(deterministic), round_tokens
+        cfg.group_bytes = group_bytes
         h = C.c_void_p()
         st = lib().fw2v_batch_create(C.byref(cfg), C.byref(h))
         if st != 0:

@@ -260,6 +260,8 @@ typedef struct fw2v_batch_config {
   int32_t use_graph;      /* 1: each fw2v_batch_train call runs as one CUDA graph */
   int32_t deterministic;  /* 1: one warp trains every round's sentences in order */
   int64_t round_tokens;   /* readable tokens sampled per round (buffer size); 0: 2^27 */
+  int64_t group_bytes;    /* table bytes of a group of jobs trained side by side; 0: half
+                             the device's L2 cache; < 0: all jobs of a family in one group */
 } fw2v_batch_config;
 
 typedef struct fw2v_batch_stats {

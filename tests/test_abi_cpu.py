@@ -53,7 +53,7 @@ def test_batch_without_device_fails_cleanly():
     assert e.value.status == 6
     cfg = fw2v.BatchConfig()
     fw2v.lib().fw2v_batch_config_default(C.byref(cfg))
-    assert (cfg.precision, cfg.use_graph, cfg.deterministic, cfg.round_tokens) == (fw2v.FP32, 1, 0, 0)
+    assert (cfg.precision, cfg.use_graph, cfg.deterministic, cfg.round_tokens, cfg.group_bytes) == (fw2v.FP32, 1, 0, 0, 0)
     bad = fw2v.BatchConfig(precision=7)
     assert fw2v.lib().fw2v_batch_create(C.byref(bad), C.byref(C.c_void_p())) == 1
 

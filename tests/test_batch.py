@@ -106,9 +106,10 @@ def jobs():
     return _jobs()
 
 
-@pytest.mark.parametrize("use_graph", [True, False])
-def test_deterministic_batch_equals_each_job_alone_fp32(jobs, use_graph):
-    with _batch(jobs, deterministic=True, use_graph=use_graph, round_tokens=3000) as b:
+# group_bytes 1: every job a group of its own; -1: all jobs interleaved
+@pytest.mark.parametrize("use_graph,group_bytes", [(True, 0), (False, 0), (True, 1), (True, -1)])
+def test_deterministic_batch_equals_each_job_alone_fp32(jobs, use_graph, group_bytes):
+    with _batch(jobs, deterministic=True, use_graph=use_graph, round_tokens=3000, group_bytes=group_bytes) as b:
         st = b.train()
         assert st.rounds > 3 and st.epochs == 3
         for j, (corpus, over) in enumerate(jobs):
@@ -118,8 +119,9 @@ def test_deterministic_batch_equals_each_job_alone_fp32(jobs, use_graph):
             assert b.job_words(j)[0] == _words(corpus, over)
 
 
-def test_deterministic_batch_equals_each_job_alone_bf16(jobs):
-    with _batch(jobs, precision=fw2v.BF16, deterministic=True, round_tokens=5000) as b:
+@pytest.mark.parametrize("group_bytes", [0, 1])
+def test_deterministic_batch_equals_each_job_alone_bf16(jobs, group_bytes):
+    with _batch(jobs, precision=fw2v.BF16, deterministic=True, round_tokens=5000, group_bytes=group_bytes) as b:
         b.train()
         for j, (corpus, over) in enumerate(jobs):
             r0, r1 = _oracle_job(corpus, over, b.shape(j), bf16=True)
