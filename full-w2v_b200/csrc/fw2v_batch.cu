@@ -262,8 +262,7 @@ void free_plan(fw2v_batch* b) {
 }
 
 int64_t shape_smem_floats(const BatchJob& j, int elem) {
-  const bool pre = j.prefetch != 0;
-  return ((int64_t)(2 * j.cfg.window + 2) * j.pitch * 4 + (int64_t)((pre ? 2 : 1) * j.stages + 2) * j.pitch * elem) / 4;
+  return warp_smem_bytes(2 * j.cfg.window + 1, j.stages, j.prefetch != 0, j.pitch, elem) / 4;
 }
 int64_t shape_scratch_elems(const BatchJob& j) { return (int64_t)(2 * j.cfg.window + 1) * j.pitch; }
 

@@ -33,7 +33,7 @@ struct BatchTrainArgs {
   void* orig_scratch;           // per warp: scratch_elems table elements
   int64_t scratch_elems;
   int64_t scratch_warps;
-  int64_t smem_floats;          // per warp: shared-memory floats (ring, sink, staging)
+  int64_t smem_floats;          // per warp: shared-memory floats (warp_smem_bytes / 4)
   const float* exp_table;
 };
 
@@ -114,7 +114,7 @@ template <typename T, int FAMILY>
 __global__ void __launch_bounds__(BatchFamily<FAMILY>::kMaxWarps * 32, BatchFamily<FAMILY>::kMinBlocks)
     sgns_batch_kernel(BatchTrainArgs a) {
   extern __shared__ __align__(16) float smem[];
-  __shared__ __align__(8) TrainParams tp[kBatchMaxWarps];
+  __shared__ __align__(8) TrainParams tp[BatchFamily<FAMILY>::kMaxWarps];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   float* ring = smem + (int64_t)warp * a.smem_floats;

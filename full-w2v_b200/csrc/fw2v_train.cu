@@ -51,11 +51,9 @@ LaunchShape choose_shape(int d, int negative) {
   return s;
 }
 
-// Shared memory of one block: per warp, the FP32 ring of 2W+1 rows and a sink
-// row, then R target rows (two sets with the prefetch) and two staging rows of
-// the table's element type (WarpRows).
+// Shared memory of one block: warp_smem_bytes per warp.
 size_t train_smem_bytes(int window, int64_t pitch, int warps, int r, bool prefetch, int elem) {
-  return (size_t)warps * ((size_t)(2 * window + 2) * pitch * 4 + (size_t)((prefetch ? 2 : 1) * r + 2) * pitch * elem);
+  return (size_t)warps * (size_t)warp_smem_bytes(2 * window + 1, r, prefetch, pitch, elem);
 }
 
 // Warps the scratch of a handle must cover: every warp the persistent grid can

@@ -63,35 +63,131 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
+// Lane layouts of up to 4 vectors per lane use ceil(d / (32 VEC)) of them,
+// so every vector but the last lies wholly inside the row on every lane: its
+// accesses need no test.  (Layouts of 6 or 8 vectors may end in vectors past
+// d; all their vectors are tested.)
+template <int VEC, int NV>
+__host__ __device__ constexpr bool head_vector(int i) {
+  return NV <= 4 && i < NV - 1;
+}
+// Vector i of a lane starting at element e: wholly inside a row of d elements.
+template <int VEC, int NV>
+__device__ __forceinline__ bool vec_whole(int i, int e, int d) {
+  return head_vector<VEC, NV>(i) || e + VEC <= d;
+}
+// ... starting inside it.
+template <int VEC, int NV>
+__device__ __forceinline__ bool vec_inside(int i, int e, int d) {
+  return head_vector<VEC, NV>(i) || e < d;
+}
+// The tail vectors of rows of several vectors per lane lie wholly inside the
+// row on some lanes and wholly past it on the others (unless d is not a
+// multiple of VEC, when one lane straddles it).  A lane accesses such a vector
+// whole or not at all under a predicate instead of a branch that would split
+// the warp; only a straddling lane takes the element path.
+template <int VEC, int NV>
+__device__ __forceinline__ bool vec_predicated(int i, int e, int d) {
+  return NV > 1 && !head_vector<VEC, NV>(i) && (e >= d || e + VEC <= d);
+}
+
+// Predicated stores and reductions: `on` selects whether the access happens.
+__device__ __forceinline__ void st_shared_u32x2_if(uint32_t a, uint32_t x, uint32_t y, bool on) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %3, 0;\n\t@q st.shared.v2.b32 [%0], {%1,%2};\n\t}" ::"r"(a),
+               "r"(x), "r"(y), "r"((int)on)
+               : "memory");
+}
+__device__ __forceinline__ void st_shared_u32_if(uint32_t a, uint32_t x, bool on) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q st.shared.b32 [%0], %1;\n\t}" ::"r"(a), "r"(x),
+               "r"((int)on)
+               : "memory");
+}
+__device__ __forceinline__ void st_global_cg_f32x4_if(float* p, float x, float y, float z, float w, bool on) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %5, 0;\n\t@q st.global.cg.v4.f32 [%0], {%1,%2,%3,%4};\n\t}" ::"l"(p),
+               "f"(x), "f"(y), "f"(z), "f"(w), "r"((int)on)
+               : "memory");
+}
+__device__ __forceinline__ void st_global_cg_f32x2_if(float* p, float x, float y, bool on) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %3, 0;\n\t@q st.global.cg.v2.f32 [%0], {%1,%2};\n\t}" ::"l"(p),
+               "f"(x), "f"(y), "r"((int)on)
+               : "memory");
+}
+__device__ __forceinline__ void st_global_cg_u32x2_if(void* p, uint32_t x, uint32_t y, bool on) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %3, 0;\n\t@q st.global.cg.v2.b32 [%0], {%1,%2};\n\t}" ::"l"(p),
+               "r"(x), "r"(y), "r"((int)on)
+               : "memory");
+}
+__device__ __forceinline__ void st_global_cg_u32_if(void* p, uint32_t x, bool on) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q st.global.cg.b32 [%0], %1;\n\t}" ::"l"(p), "r"(x),
+               "r"((int)on)
+               : "memory");
+}
+__device__ __forceinline__ void red_add_f32x4_if(float* p, float x, float y, float z, float w, bool on) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %5, 0;\n\t@q red.global.add.v4.f32 [%0], {%1,%2,%3,%4};\n\t}" ::"l"(p),
+               "f"(x), "f"(y), "f"(z), "f"(w), "r"((int)on)
+               : "memory");
+}
+__device__ __forceinline__ void red_add_f32x2_if(float* p, float x, float y, bool on) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %3, 0;\n\t@q red.global.add.v2.f32 [%0], {%1,%2};\n\t}" ::"l"(p),
+               "f"(x), "f"(y), "r"((int)on)
+               : "memory");
+}
+__device__ __forceinline__ void red_add_bf16x2x2_if(void* p, uint32_t x, uint32_t y, bool on) {
+  asm volatile(
+      "{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %3, 0;\n\t@q red.global.add.noftz.v2.bf16x2 [%0], {%1,%2};\n\t}" ::"l"(p),
+      "r"(x), "r"(y), "r"((int)on)
+      : "memory");
+}
+__device__ __forceinline__ void red_add_bf16x2_if(void* p, uint32_t x, bool on) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q red.global.add.noftz.bf16x2 [%0], %1;\n\t}" ::"l"(p),
+               "r"(x), "r"((int)on)
+               : "memory");
+}
+
 template <int VEC, int NV>
 struct LaneMap {
   uint32_t off[NV];  // byte offset of this lane's vector i within a row
   bool ok[NV];       // vector i starts inside the row (e < d)
-  __device__ __forceinline__ LaneMap(int lane, int d) {
+  uint32_t zero;     // a 16-byte zero vector in shared memory, read in place of vectors past d
+  __device__ __forceinline__ LaneMap(int lane, int d, uint32_t zero_b) : zero(zero_b) {
 #pragma unroll
     for (int i = 0; i < NV; i++) {
       const int e = (i * 32 + lane) * VEC;
       off[i] = (uint32_t)e * 4u;
-      ok[i] = e < d;
+      ok[i] = head_vector<VEC, NV>(i) || e < d;
     }
+  }
+  // shared-memory address of vector i of a row for a load: the zero vector
+  // past d
+  __device__ __forceinline__ uint32_t ld_addr(uint32_t row, int i) const {
+    if (head_vector<VEC, NV>(i)) return row + off[i];
+    return ok[i] ? row + off[i] : zero;
   }
 };
 
+// Rows of one vector per lane (d <= 128) test the lane with a branch, which
+// is the same on every lane when d fills the warp.  The last vector of wider
+// rows, which ends inside the row on some lanes only, is loaded from the zero
+// vector and stored under a predicate instead: a branch that splits the warp
+// costs more than the select.
 template <int VEC, int NV>
 __device__ __forceinline__ void lds_row(Row<VEC, NV>& r, uint32_t row, const LaneMap<VEC, NV>& m) {
 #pragma unroll
   for (int i = 0; i < NV; i++) {
     if constexpr (VEC == 4) {
-      float a = 0.f, b = 0.f, c = 0.f, e = 0.f;
-      if (m.ok[i])
-        asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
-                     : "=f"(a), "=f"(b), "=f"(c), "=f"(e)
-                     : "r"(row + m.off[i]));
-      r.x[i][0] = a; r.x[i][1] = b; r.x[i][2] = c; r.x[i][3] = e;
+      if (NV == 1 && !m.ok[i]) {
+        r.x[i][0] = r.x[i][1] = r.x[i][2] = r.x[i][3] = 0.0f;
+        continue;
+      }
+      asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
+                   : "=f"(r.x[i][0]), "=f"(r.x[i][1]), "=f"(r.x[i][2]), "=f"(r.x[i][3])
+                   : "r"(m.ld_addr(row, i)));
     } else {
-      float a = 0.f, b = 0.f;
-      if (m.ok[i]) asm volatile("ld.shared.v2.f32 {%0,%1}, [%2];" : "=f"(a), "=f"(b) : "r"(row + m.off[i]));
-      r.x[i][0] = a; r.x[i][1] = b;
+      if (NV == 1 && !m.ok[i]) {
+        r.x[i][0] = r.x[i][1] = 0.0f;
+        continue;
+      }
+      asm volatile("ld.shared.v2.f32 {%0,%1}, [%2];" : "=f"(r.x[i][0]), "=f"(r.x[i][1]) : "r"(m.ld_addr(row, i)));
     }
   }
 }
@@ -100,15 +196,25 @@ template <int VEC, int NV>
 __device__ __forceinline__ void sts_row(const Row<VEC, NV>& r, uint32_t row, const LaneMap<VEC, NV>& m) {
 #pragma unroll
   for (int i = 0; i < NV; i++) {
-    if (m.ok[i]) {
-      if constexpr (VEC == 4) {
-        asm volatile("st.shared.v4.f32 [%0], {%1,%2,%3,%4};" ::"r"(row + m.off[i]), "f"(r.x[i][0]),
-                     "f"(r.x[i][1]), "f"(r.x[i][2]), "f"(r.x[i][3])
+    const uint32_t a = row + m.off[i];
+    if (head_vector<VEC, NV>(i) || NV == 1) {
+      if (NV == 1 && !m.ok[i]) continue;
+      if constexpr (VEC == 4)
+        asm volatile("st.shared.v4.f32 [%0], {%1,%2,%3,%4};" ::"r"(a), "f"(r.x[i][0]), "f"(r.x[i][1]),
+                     "f"(r.x[i][2]), "f"(r.x[i][3])
                      : "memory");
-      } else {
-        asm volatile("st.shared.v2.f32 [%0], {%1,%2};" ::"r"(row + m.off[i]), "f"(r.x[i][0]), "f"(r.x[i][1])
+      else
+        asm volatile("st.shared.v2.f32 [%0], {%1,%2};" ::"r"(a), "f"(r.x[i][0]), "f"(r.x[i][1]) : "memory");
+    } else {
+      const int on = m.ok[i];
+      if constexpr (VEC == 4)
+        asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %5, 0;\n\t@q st.shared.v4.f32 [%0], {%1,%2,%3,%4};\n\t}"
+                     ::"r"(a), "f"(r.x[i][0]), "f"(r.x[i][1]), "f"(r.x[i][2]), "f"(r.x[i][3]), "r"(on)
                      : "memory");
-      }
+      else
+        asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %3, 0;\n\t@q st.shared.v2.f32 [%0], {%1,%2};\n\t}"
+                     ::"r"(a), "f"(r.x[i][0]), "f"(r.x[i][1]), "r"(on)
+                     : "memory");
     }
   }
 }
@@ -119,9 +225,19 @@ template <int VEC, int NV>
 __device__ __forceinline__ void cp_row(uint32_t dst, const float* src, const LaneMap<VEC, NV>& m, int d) {
 #pragma unroll
   for (int i = 0; i < NV; i++) {
-    if (m.ok[i]) {
+    const int e0 = (int)(m.off[i] / 4);
+    if (vec_predicated<VEC, NV>(i, e0, d)) {
+      // whole, or a zero-byte copy (zero fill) into the zero vector
+      const bool on = e0 < d;
+      const uint32_t da = on ? dst + m.off[i] : m.zero;
+      const float* g = on ? src + e0 : src;
+      if constexpr (VEC == 4)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(da), "l"(g), "r"(on ? 16 : 0) : "memory");
+      else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(da), "l"(g), "r"(on ? 8 : 0) : "memory");
+    } else if (m.ok[i]) {
       const float* g = src + m.off[i] / 4;
-      if ((int)(m.off[i] / 4) + VEC <= d) {
+      if (vec_whole<VEC, NV>(i, (int)(m.off[i] / 4), d)) {
         if constexpr (VEC == 4)
           asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + m.off[i]), "l"(g) : "memory");
         else
@@ -163,7 +279,18 @@ __device__ __forceinline__ void row_load_global(Row<VEC, NV>& r, const float* ro
 #pragma unroll
   for (int i = 0; i < NV; i++) {
     const int e = (i * 32 + lane) * VEC;
-    if (e + VEC <= d) {
+    if (vec_predicated<VEC, NV>(i, e, d)) {
+      const bool on = e < d;
+      const float* g = row + (on ? e : 0);
+      if constexpr (VEC == 4) {
+        const float4 t = __ldcg(reinterpret_cast<const float4*>(g));
+        r.x[i][0] = on ? t.x : 0.0f; r.x[i][1] = on ? t.y : 0.0f;
+        r.x[i][2] = on ? t.z : 0.0f; r.x[i][3] = on ? t.w : 0.0f;
+      } else {
+        const float2 t = __ldcg(reinterpret_cast<const float2*>(g));
+        r.x[i][0] = on ? t.x : 0.0f; r.x[i][1] = on ? t.y : 0.0f;
+      }
+    } else if (vec_whole<VEC, NV>(i, e, d)) {
       if constexpr (VEC == 4) {
         const float4 t = __ldcg(reinterpret_cast<const float4*>(row + e));
         r.x[i][0] = t.x; r.x[i][1] = t.y; r.x[i][2] = t.z; r.x[i][3] = t.w;
@@ -183,7 +310,7 @@ __device__ __forceinline__ void row_load_smem(Row<VEC, NV>& r, const float* row,
 #pragma unroll
   for (int i = 0; i < NV; i++) {
     const int e = (i * 32 + lane) * VEC;
-    if (e < d) {
+    if (vec_inside<VEC, NV>(i, e, d)) {
       if constexpr (VEC == 4) {
         const float4 t = *reinterpret_cast<const float4*>(row + e);
         r.x[i][0] = t.x; r.x[i][1] = t.y; r.x[i][2] = t.z; r.x[i][3] = t.w;
@@ -203,7 +330,7 @@ __device__ __forceinline__ void row_store_smem(const Row<VEC, NV>& r, float* row
 #pragma unroll
   for (int i = 0; i < NV; i++) {
     const int e = (i * 32 + lane) * VEC;
-    if (e < d) {
+    if (vec_inside<VEC, NV>(i, e, d)) {
       if constexpr (VEC == 4) {
         *reinterpret_cast<float4*>(row + e) = make_float4(r.x[i][0], r.x[i][1], r.x[i][2], r.x[i][3]);
       } else {
@@ -221,7 +348,13 @@ __device__ __forceinline__ void row_add_delta(float* row, const Row<VEC, NV>& a,
 #pragma unroll
   for (int i = 0; i < NV; i++) {
     const int e = (i * 32 + lane) * VEC;
-    if (e + VEC <= d) {
+    if (vec_predicated<VEC, NV>(i, e, d)) {
+      if constexpr (VEC == 4)
+        red_add_f32x4_if(row + e, __fsub_rn(a.x[i][0], b.x[i][0]), __fsub_rn(a.x[i][1], b.x[i][1]),
+                         __fsub_rn(a.x[i][2], b.x[i][2]), __fsub_rn(a.x[i][3], b.x[i][3]), e < d);
+      else
+        red_add_f32x2_if(row + e, __fsub_rn(a.x[i][0], b.x[i][0]), __fsub_rn(a.x[i][1], b.x[i][1]), e < d);
+    } else if (vec_whole<VEC, NV>(i, e, d)) {
       if constexpr (VEC == 4) {
         const float4 dlt = make_float4(__fsub_rn(a.x[i][0], b.x[i][0]), __fsub_rn(a.x[i][1], b.x[i][1]),
                                        __fsub_rn(a.x[i][2], b.x[i][2]), __fsub_rn(a.x[i][3], b.x[i][3]));
@@ -249,7 +382,21 @@ __device__ __forceinline__ void row_load_global(Row<VEC, NV>& r, const bf16_t* r
 #pragma unroll
   for (int i = 0; i < NV; i++) {
     const int e = (i * 32 + lane) * VEC;
-    if (e + VEC <= d) {
+    if (vec_predicated<VEC, NV>(i, e, d)) {
+      const bool on = e < d;
+      const uint16_t* g = h + (on ? e : 0);
+      if constexpr (VEC == 4) {
+        uint2 t = __ldcg(reinterpret_cast<const uint2*>(g));
+        t.x = on ? t.x : 0u;
+        t.y = on ? t.y : 0u;
+        r.x[i][0] = bf16_value((uint16_t)t.x); r.x[i][1] = bf16_value((uint16_t)(t.x >> 16));
+        r.x[i][2] = bf16_value((uint16_t)t.y); r.x[i][3] = bf16_value((uint16_t)(t.y >> 16));
+      } else {
+        unsigned t = __ldcg(reinterpret_cast<const unsigned*>(g));
+        t = on ? t : 0u;
+        r.x[i][0] = bf16_value((uint16_t)t); r.x[i][1] = bf16_value((uint16_t)(t >> 16));
+      }
+    } else if (vec_whole<VEC, NV>(i, e, d)) {
       if constexpr (VEC == 4) {
         const uint2 t = __ldcg(reinterpret_cast<const uint2*>(h + e));
         r.x[i][0] = bf16_value((uint16_t)t.x); r.x[i][1] = bf16_value((uint16_t)(t.x >> 16));
@@ -288,9 +435,20 @@ __device__ __forceinline__ void row_add_delta(bf16_t* row, const Row<VEC, NV>& a
 #pragma unroll
   for (int i = 0; i < NV; i++) {
     const int e = (i * 32 + lane) * VEC;
-    if (e >= d) continue;
+    if (vec_predicated<VEC, NV>(i, e, d)) {
+      const uint64_t bits = sr_vector_bits(key, row_id, (uint64_t)(e / VEC));
+      const uint32_t p0 = sr_increment2(a.x[i][0], b.x[i][0], a.x[i][1], b.x[i][1], (uint32_t)bits);
+      if constexpr (VEC == 4) {
+        const uint32_t p1 = sr_increment2(a.x[i][2], b.x[i][2], a.x[i][3], b.x[i][3], (uint32_t)(bits >> 32));
+        red_add_bf16x2x2_if(h + e, p0, p1, e < d);
+      } else {
+        red_add_bf16x2_if(h + e, p0, e < d);
+      }
+      continue;
+    }
+    if (!vec_inside<VEC, NV>(i, e, d)) continue;
     const uint64_t bits = sr_vector_bits(key, row_id, (uint64_t)(e / VEC));
-    if (e + VEC <= d) {
+    if (vec_whole<VEC, NV>(i, e, d)) {
       const uint32_t p0 = sr_increment2(a.x[i][0], b.x[i][0], a.x[i][1], b.x[i][1], (uint32_t)bits);
       if constexpr (VEC == 4) {
         const uint32_t p1 = sr_increment2(a.x[i][2], b.x[i][2], a.x[i][3], b.x[i][3], (uint32_t)(bits >> 32));
@@ -478,7 +636,12 @@ __device__ __forceinline__ void row_store_global(const Row<VEC, NV>& r, float* r
 #pragma unroll
   for (int i = 0; i < NV; i++) {
     const int e = (i * 32 + lane) * VEC;
-    if (e < d) {
+    if (vec_predicated<VEC, NV>(i, e, d)) {
+      if constexpr (VEC == 4)
+        st_global_cg_f32x4_if(row + e, r.x[i][0], r.x[i][1], r.x[i][2], r.x[i][3], e < d);
+      else
+        st_global_cg_f32x2_if(row + e, r.x[i][0], r.x[i][1], e < d);
+    } else if (vec_inside<VEC, NV>(i, e, d)) {
       if constexpr (VEC == 4) {
         __stcg(reinterpret_cast<float4*>(row + e), make_float4(r.x[i][0], r.x[i][1], r.x[i][2], r.x[i][3]));
       } else {
@@ -494,7 +657,15 @@ __device__ __forceinline__ void row_store_global(const Row<VEC, NV>& r, bf16_t* 
 #pragma unroll
   for (int i = 0; i < NV; i++) {
     const int e = (i * 32 + lane) * VEC;
-    if (e + VEC <= d) {
+    if (vec_predicated<VEC, NV>(i, e, d)) {
+      const uint32_t x = (unsigned)bf16_nearest(r.x[i][0]) | ((unsigned)bf16_nearest(r.x[i][1]) << 16);
+      if constexpr (VEC == 4) {
+        const uint32_t y = (unsigned)bf16_nearest(r.x[i][2]) | ((unsigned)bf16_nearest(r.x[i][3]) << 16);
+        st_global_cg_u32x2_if(h + e, x, y, e < d);
+      } else {
+        st_global_cg_u32_if(h + e, x, e < d);
+      }
+    } else if (vec_whole<VEC, NV>(i, e, d)) {
       if constexpr (VEC == 4) {
         uint2 t;
         t.x = (unsigned)bf16_nearest(r.x[i][0]) | ((unsigned)bf16_nearest(r.x[i][1]) << 16);
@@ -518,10 +689,22 @@ __device__ __forceinline__ void cp_row(uint32_t dst, const bf16_t* src, const La
   const uint16_t* h = reinterpret_cast<const uint16_t*>(src);
 #pragma unroll
   for (int i = 0; i < NV; i++) {
+    const int e0 = (int)(m.off[i] / 4);
+    if (vec_predicated<VEC, NV>(i, e0, d)) {
+      // whole, or a zero-byte copy (zero fill) into the zero vector
+      const bool on = e0 < d;
+      const uint32_t da = on ? dst + (uint32_t)e0 * 2u : m.zero;
+      const uint16_t* g = on ? h + e0 : h;
+      if constexpr (VEC == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(da), "l"(g), "r"(on ? 8 : 0) : "memory");
+      else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(da), "l"(g), "r"(on ? 4 : 0) : "memory");
+      continue;
+    }
     if (!m.ok[i]) continue;
-    const int e = (int)(m.off[i] / 4);
+    const int e = e0;
     const uint32_t da = dst + (uint32_t)e * 2u;
-    if (e + VEC <= d) {
+    if (vec_whole<VEC, NV>(i, e, d)) {
       if constexpr (VEC == 4)
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(da), "l"(h + e) : "memory");
       else
@@ -541,8 +724,8 @@ __device__ __forceinline__ void lds_row_bf16(Row<VEC, NV>& r, uint32_t row, cons
 #pragma unroll
   for (int i = 0; i < NV; i++) {
     unsigned a = 0, b = 0;
-    const uint32_t at = row + (m.off[i] / 4) * 2u;
-    if (m.ok[i]) {
+    if (NV > 1 || m.ok[i]) {
+      const uint32_t at = head_vector<VEC, NV>(i) || m.ok[i] ? row + (m.off[i] / 4) * 2u : m.zero;
       if constexpr (VEC == 4) asm volatile("ld.shared.v2.u32 {%0,%1}, [%2];" : "=r"(a), "=r"(b) : "r"(at));
       else asm volatile("ld.shared.u32 %0, [%1];" : "=r"(a) : "r"(at));
     }
@@ -572,36 +755,38 @@ __device__ __forceinline__ void sts_staged(const Row<VEC, NV>& r, uint32_t row, 
   } else {
 #pragma unroll
     for (int i = 0; i < NV; i++) {
-      if (!m.ok[i]) continue;
+      const bool pred = NV > 1 && !head_vector<VEC, NV>(i);  // stored under a predicate, no branch
+      if (!pred && !m.ok[i]) continue;
       const uint32_t at = row + (m.off[i] / 4) * 2u;
       const uint32_t a = __byte_perm(__float_as_uint(r.x[i][0]), __float_as_uint(r.x[i][1]), 0x7632);
       if constexpr (VEC == 4) {
         const uint32_t b = __byte_perm(__float_as_uint(r.x[i][2]), __float_as_uint(r.x[i][3]), 0x7632);
-        asm volatile("st.shared.v2.u32 [%0], {%1, %2};" ::"r"(at), "r"(a), "r"(b) : "memory");
+        if (pred) st_shared_u32x2_if(at, a, b, m.ok[i]);
+        else asm volatile("st.shared.v2.u32 [%0], {%1, %2};" ::"r"(at), "r"(a), "r"(b) : "memory");
       } else {
-        asm volatile("st.shared.u32 [%0], %1;" ::"r"(at), "r"(a) : "memory");
+        if (pred) st_shared_u32_if(at, a, m.ok[i]);
+        else asm volatile("st.shared.u32 [%0], %1;" ::"r"(at), "r"(a) : "memory");
       }
     }
   }
 }
 
-// Shared-memory rows of one warp, each `P` floats.
-template <int R>
-struct WarpRows {
-  // FP32 ring and sink rows, then staged rows of the table's element type: R
-  // target originals (2 x R with the target prefetch) and 2 staging rows
-  __host__ __device__ static constexpr int64_t bytes(int D, bool prefetch, int64_t pitch, int elem) {
-    return (int64_t)(D + 1) * pitch * 4 + (int64_t)((prefetch ? 2 : 1) * R + 2) * pitch * elem;
-  }
-};
+// Shared memory of one warp, rows of `pitch` elements: the FP32 ring of
+// D = 2W+1 rows and a sink row, then staged rows of the table's element type
+// (R target originals, 2 x R with the target prefetch, and 2 staging rows),
+// then a 16-byte zero vector.
+__host__ __device__ constexpr int64_t warp_smem_bytes(int D, int R, bool prefetch, int64_t pitch, int elem) {
+  return (int64_t)(D + 1) * pitch * 4 + (int64_t)((prefetch ? 2 : 1) * R + 2) * pitch * elem + 16;
+}
 
 // One sentence on one warp.
-//   ring     shared memory (WarpRows<R>::rows rows): slot p % D holds the
-//            current value of sentence position p while it is in the window;
-//            slot D is a sink that the pipeline reads and writes on its idle
-//            steps; then the R target rows as loaded (for their write-back) and
-//            two staging rows filled by cp.async (the entering row and the
-//            leaving row's original value).
+//   ring     shared memory (warp_smem_bytes): slot p % D holds the current
+//            value of sentence position p while it is in the window; slot D
+//            is a sink that the pipeline reads and writes on its idle steps;
+//            then the R target rows as loaded (for their write-back), two
+//            staging rows filled by cp.async (the entering row and the leaving
+//            row's original value) and the zero vector that lanes read in
+//            place of vectors past d.
 //   orig     this warp's global scratch, D rows: the value each slot's row had
 //            when it entered the window (needed for its single write-back).
 template <typename T, int VEC, int NV, int R, int SIG>
@@ -644,7 +829,6 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
     row_store_smem(tmp, ring + q * P, lane, d);
     row_store_global(tmp, orig + q * P, lane, d);
   }
-  const LaneMap<VEC, NV> lm(lane, d);
   const uint32_t ring_b = smem_addr(ring);
   const uint32_t row_bytes = (uint32_t)P * 4u;
   // staged rows (target originals, entering and leaving copies) hold the
@@ -661,6 +845,10 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   const uint32_t o1_b = o0_b + (uint32_t)R * srow_bytes;
   const uint32_t in_b = pre ? o1_b + (uint32_t)R * srow_bytes : o1_b;
   const uint32_t out_b = in_b + srow_bytes;
+  const uint32_t zero_b = out_b + srow_bytes;
+  if (lane < 4) asm volatile("st.shared.f32 [%0], %1;" ::"r"(zero_b + 4u * lane), "f"(0.0f) : "memory");
+  __syncwarp();
+  const LaneMap<VEC, NV> lm(lane, d, zero_b);
   auto prefetch_targets = [&](uint32_t set, int my_target, int n) {
     for (int k = 0; k < n; k++) {
       const int tk = __shfl_sync(kFull, my_target, k);
@@ -690,6 +878,11 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
     cp_async_commit();
   }
   int t_prev = -1;  // lane k < R: target k of the previous group of targets (written back), else -1
+  // The ring slot of position w - W, which leaves at centre w and whose slot
+  // position w + W + 1 takes ((w - W) mod D), and on lane r < D the offset of
+  // slot r from it ((r - (w - W)) mod D): both move by one slot per centre.
+  int slot_out = W + 1 < D ? W + 1 : 0;
+  int lane_off = lane + W < D ? lane + W : lane + W - D;
   for (int w = 0; w < L; w++) {
     // Ids and rows needed later in this centre, loaded ahead of use.
     const int q_out = w - W, q_in = w + W + 1;
@@ -702,15 +895,14 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
     // in the background while the centre trains.
     const bool enter_early = id_in >= 0 && id_in != id_out;
     if (enter_early) cp_row(in_b, syn0 + (int64_t)id_in * P, lm, d);
-    if (q_out >= 0) cp_row(out_b, orig + (q_out % D) * P, lm, d);
+    if (q_out >= 0) cp_row(out_b, orig + slot_out * P, lm, d);
     cp_async_commit();
 
     // Lane r < D decides whether ring slot r holds a context of centre w.
     const int base = w - W;
     bool valid = false;
     if (lane < D) {
-      const int off = ((lane - base) % D + D) % D;
-      const int pos = base + off;
+      const int pos = base + lane_off;
       valid = pos != w && pos >= 0 && pos < L;
     }
     const unsigned mask = __ballot_sync(kFull, valid);
@@ -855,19 +1047,21 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
     else cp_async_wait();
     if (q_out >= 0) {
       Row<VEC, NV> cur, org;
-      lds_row(cur, ring_b + (uint32_t)(q_out % D) * row_bytes, lm);
+      lds_row(cur, ring_b + (uint32_t)slot_out * row_bytes, lm);
       lds_staged<T>(org, out_b, lm);
       row_add_delta(syn0 + (int64_t)id_out * P, cur, org, lane, d,
                     sr_event_key(skey, (uint64_t)L * (K + 1) + q_out), (uint64_t)id_out);
     }
     if (id_in >= 0) {
-      const int s = q_in % D;
+      const int s = slot_out;
       Row<VEC, NV> enter_row;
       if (enter_early) lds_staged<T>(enter_row, in_b, lm);
       else row_load_global(enter_row, syn0 + (int64_t)id_in * P, lane, d);
       sts_row(enter_row, ring_b + (uint32_t)s * row_bytes, lm);
       row_store_global(enter_row, orig + s * P, lane, d);
     }
+    slot_out = slot_out + 1 < D ? slot_out + 1 : 0;
+    lane_off = lane_off > 0 ? lane_off - 1 : D - 1;
   }
   // Positions still in the window leave in increasing order.
   for (int q = L - W > 0 ? L - W : 0; q < L; q++) {
@@ -902,8 +1096,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MinBlocks<NV>::value) sgn
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int D = 2 * p.window + 1;
-  float* ring = smem + (int64_t)warp *
-                           WarpRows<R>::bytes(D, p.prefetch != 0, p.pitch, (int)sizeof(T)) / 4;
+  float* ring = smem + (int64_t)warp * warp_smem_bytes(D, R, p.prefetch != 0, p.pitch, (int)sizeof(T)) / 4;
   const int64_t gwarp = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
   T* orig = reinterpret_cast<T*>(p.orig_scratch) + gwarp * D * p.pitch;
   const int64_t total = total_sentences(p);
