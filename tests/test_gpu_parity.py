@@ -105,9 +105,12 @@ def _flatten_epoch(out, e):
     return lens, alphas, ids, negs
 
 
+# 301: a lane straddles d in the last vector; 500: four vectors per lane;
+# 600: six, the last wholly past d on every lane
 @pytest.mark.parametrize("name,d", [("zipf_t1", 8), ("zipf_t1", 100), ("eos_t1", 128),
                                     ("zipf_t3", 300), ("k0_t1", 64), ("messy_t1", 40),
-                                    ("nosample_t2", 200)])
+                                    ("nosample_t2", 200), ("zipf_t1", 301), ("eos_t1", 500),
+                                    ("zipf_t1", 600)])
 def test_deterministic_training_bit_exact_fp32_table_sigmoid(name, d):
     g = load(name)
     c = dict(g["cfg"])
@@ -308,7 +311,8 @@ def _first_launch_seed():
     return O.mix64(0x5EEDF00D)
 
 
-@pytest.mark.parametrize("name,d", [("zipf_t1", 128), ("eos_t1", 100), ("zipf_t3", 300), ("k0_t1", 64)])
+@pytest.mark.parametrize("name,d", [("zipf_t1", 128), ("eos_t1", 100), ("zipf_t3", 300), ("k0_t1", 64),
+                                    ("zipf_t1", 301)])
 def test_deterministic_bf16_epoch_bit_exact(name, d):
     """Same sampler, FP32 math in the kernel's order, and the same counter-based
     stochastic rounding as the oracle: the tables agree bit for bit."""
