@@ -1,4 +1,4 @@
-"""Embedding quality on the synthetic corpora (the reference judges quality with
+"""Embedding quality on the synthetic corpora (the reference measures quality with
 public word-similarity sets under analysis/hyperwords/, which are not available
 offline).
 

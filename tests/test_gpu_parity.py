@@ -5,8 +5,8 @@ match bit for bit.  The training update is checked in deterministic mode:
   * table sigmoid against the oracle's FP32 mode, which reproduces the kernel's
     operation order: bit for bit;
   * exact sigmoid against the oracle's FP64 mode: max |gpu - fp64| <= 1e-5 *
-    max|fp64| per table (the tolerance of the north-star spec, "within 1e-5
-    relative").
+    max|fp64| per table (the required tolerance: "within 1e-5 relative" of
+    FP64).
 """
 import hashlib
 
