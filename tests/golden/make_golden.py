@@ -3,7 +3,8 @@
 Run from the repository root in a container that has the reference checkout:
 
     make -C oracle ref          # builds oracle/_ref/fw2v_ref_host from the reference sources
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every fixture
+    python tests/golden/make_golden.py --shape    # only the benchmark-shaped digests
 
 ``oracle/_ref/fw2v_ref_host`` is FULL-W2V-driver.cu (with the two .cpp files it
 includes) compiled unmodified and linked against a host-memory CUDA-runtime
@@ -15,11 +16,15 @@ initial vectors (-binary 1, untrained because the kernel is a no-op) and its
 "Overall Words" count, these pin the oracle and the CUDA sampler bit for bit.
 
 Each fixture stores the synthetic corpus it was made from (seeded generator,
-written here), the command-line flags, and the reference's outputs.
+written here), the command-line flags, and the reference's outputs.  The
+benchmark-shaped cases of tests/shape_cases.py (corpora of 1M to 12.5M tokens,
+up to 3125 sampling threads) store digests of the same outputs instead, in
+shape_<name>.json.
 """
 from __future__ import annotations
 
 import hashlib
+import json
 import os
 import shutil
 import subprocess
@@ -204,11 +209,73 @@ CASES = [
 ]
 
 
+def run_shape_case(name: str):
+    """A benchmark-shaped case (tests/shape_cases.py): the reference's batches
+    and files reduced to digests, written to shape_<name>.json."""
+    sys.path[:0] = [os.path.join(ROOT, "tests"), os.path.join(ROOT, "full-w2v_b200")]
+    import shape_cases as S
+    from fw2v import synth
+
+    case = S.CASES[name]
+    raw, ends, _ = S.raw_tokens(name)
+    text = synth.text_of(raw, ends)
+    tmp = tempfile.mkdtemp(prefix="fw2v_golden_")
+    try:
+        corpus = os.path.join(tmp, "corpus.txt")
+        with open(corpus, "wb") as f:
+            f.write(text)
+        dump = os.path.join(tmp, "dump")
+        os.mkdir(dump)
+        vec = os.path.join(tmp, "out.vec")
+        vocab = os.path.join(tmp, "out.vocab")
+        cmd = [HARNESS, "-train", corpus, "-output", vec, "-save-vocab", vocab, "-debug", "0",
+               "-binary", "1", "-streams", "1", "-kernel-batch-size", "4"] + case["flags"].split()
+        if case.get("no_export"):
+            cmd.append("-no-export")
+        r = subprocess.run(cmd, env=dict(os.environ, FW2V_REF_DUMP_DIR=dump),
+                           capture_output=True, check=True, text=True)
+        overall = [ln for ln in r.stdout.splitlines() if ln.startswith("Overall Words:")]
+        vocab_bytes = open(vocab, "rb").read()
+        per = [parse_dump(os.path.join(dump, f)) for f in sorted(os.listdir(dump))]
+        out = {
+            "name": name,
+            "generator": case["gen"],
+            "flags": case["flags"],
+            "text_sha256": hashlib.sha256(text).hexdigest(),
+            "vocab_sha256": hashlib.sha256(vocab_bytes).hexdigest(),
+            "vocab_size": vocab_bytes.count(b"\n"),
+            "overall_words": int(overall[0].split(":")[1]),
+            "streams": S.digests([(l, a, i, n) for l, a, i, n in per]),
+        }
+        if not case.get("no_export"):
+            raw_vec = open(vec, "rb").read()
+            hdr, rest = raw_vec.split(b"\n", 1)
+            V, d = (int(x) for x in hdr.split())
+            rows, p = [], 0
+            for _ in range(V):
+                p = rest.index(b" ", p) + 1
+                rows.append(np.frombuffer(rest[p:p + 4 * d], np.float32))
+                p += 4 * d + 1
+            out["syn0_init_sha256"] = hashlib.sha256(np.stack(rows).tobytes()).hexdigest()
+        with open(os.path.join(OUT, f"shape_{name}.json"), "w") as f:
+            json.dump(out, f, separators=(",", ":"))
+        print(f"shape_{name}: V={out['vocab_size']} overall_words={out['overall_words']} "
+              f"threads={len(per)} kept={sum(s[3] for s in out['streams'])}")
+    finally:
+        shutil.rmtree(tmp)
+
+
 def main():
     if not os.path.exists(HARNESS):
         sys.exit(f"missing {HARNESS}: run `make -C oracle ref` first")
-    for name, gen, flags in CASES:
-        run_case(name, gen(), flags.split())
+    only_shapes = "--shape" in sys.argv[1:]
+    if not only_shapes:
+        for name, gen, flags in CASES:
+            run_case(name, gen(), flags.split())
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import shape_cases
+    for name in shape_cases.CASES:
+        run_shape_case(name)
 
 
 if __name__ == "__main__":
