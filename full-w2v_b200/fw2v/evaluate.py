@@ -9,7 +9,8 @@ with subsampling off and fixed LCG streams, so two models are scored on
 identical pairs.
 
 precision_at_10: for query words, the share of their 10 nearest neighbours by
-cosine similarity (syn0) that share their planted topic or block.
+cosine similarity (syn0) that share their planted topic or block; the
+neighbour search is this library's kernel (fw2v_neighbours).
 """
 from __future__ import annotations
 
@@ -57,28 +58,49 @@ def heldout_loss(trainer: Trainer, pairs) -> float:
     return total / max(n, 1)
 
 
+def neighbours(table, cand: np.ndarray, queries: np.ndarray, k: int = 10, *, precision: int = 0,
+               layer_size: int | None = None, device="cuda"):
+    """The k nearest other candidates of each query by cosine similarity
+    (fw2v_neighbours, this library's kernel): (indices into cand [n_q, k],
+    cosines [n_q, k]).  `table`: rows of FP32 (or bfloat16 bits, precision
+    BF16) as a numpy array or a device tensor."""
+    import torch
+
+    from . import lib
+    t = table if isinstance(table, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(table))
+    t = t.to(device)
+    d = layer_size or t.shape[1]
+    c = torch.from_numpy(np.ascontiguousarray(cand, np.int32)).to(device)
+    q = torch.from_numpy(np.ascontiguousarray(queries, np.int32)).to(device)
+    out_i = torch.empty((len(queries), k), dtype=torch.int32, device=device)
+    out_s = torch.empty((len(queries), k), dtype=torch.float32, device=device)
+    stream = torch.cuda.current_stream(t.device)
+    st = lib().fw2v_neighbours(t.data_ptr(), precision, t.stride(0), d, c.data_ptr(), len(cand), q.data_ptr(),
+                               len(queries), k, out_i.data_ptr(), out_s.data_ptr(), stream.cuda_stream)
+    if st != 0:
+        raise RuntimeError(f"fw2v_neighbours failed: status {st}")
+    stream.synchronize()
+    return out_i.cpu().numpy(), out_s.cpu().numpy()
+
+
 def precision_at_10(syn0: np.ndarray, label: np.ndarray, counts: np.ndarray, *, purity=None,
                     min_purity: float = 0.5, queries: int = 2000, min_count: int = 5, seed: int = 0,
                     device="cuda") -> tuple[float, int]:
     """Same-label precision@10 by cosine similarity over the words that carry
     their planted label (purity above min_purity, count at least min_count):
-    queries are drawn from them and neighbours searched among them.  Returns
-    (precision, number of such words)."""
-    import torch
-
+    queries are drawn from them (all of them with queries=0) and neighbours
+    searched among all of them by this library's kernel (fw2v_neighbours).
+    Returns (precision, number of such words)."""
     ok = (label >= 0) & (counts >= min_count)
     if purity is not None:
         ok &= purity > min_purity
     cand = np.nonzero(ok)[0]
     if len(cand) < 11:
         return float("nan"), len(cand)
-    rng = np.random.default_rng(seed)
-    q = rng.choice(len(cand), size=min(queries, len(cand)), replace=False)
-    E = torch.from_numpy(np.ascontiguousarray(syn0[cand], np.float32)).to(device)
-    E = E / E.norm(dim=1, keepdim=True).clamp_min(1e-12)
-    qi = torch.from_numpy(q).to(device)
-    sims = E[qi] @ E.T
-    sims[torch.arange(len(q), device=device), qi] = -2.0
-    top = torch.topk(sims, 10, dim=1).indices.cpu().numpy()
+    if queries and queries < len(cand):
+        q = np.random.default_rng(seed).choice(len(cand), size=queries, replace=False)
+    else:
+        q = np.arange(len(cand))
+    top, _ = neighbours(syn0, cand, q, 10, device=device)
     lab = label[cand]
     return float((lab[top] == lab[q][:, None]).mean()), len(cand)
