@@ -20,13 +20,33 @@ import numpy as np
 class SynthCorpus:
     counts: np.ndarray       # uint32, vocab order, index 0 = </s>
     train_words: int
-    stream: np.ndarray       # int32 vocab ids, trailing 0
-    chunk_off: np.ndarray    # int64
+    stream: object           # int32 vocab ids, trailing 0: numpy, or a CUDA tensor (device generators)
+    chunk_off: object        # int64 chunk starts: numpy, or a CUDA tensor
     label: np.ndarray        # planted topic/block per vocab id (-1 for </s>)
     raw_of_vocab: np.ndarray  # raw id per vocab id (-1 for </s>)
     # share of a word's expected count that its planted topic contributes
     # (1 for graph nodes); words above 1/2 carry a recoverable planted label
     purity: np.ndarray | None = None
+
+    def host_stream(self) -> np.ndarray:
+        """The token stream in host memory (copied once from the device)."""
+        if not isinstance(self.stream, np.ndarray):
+            self.stream_host = getattr(self, "stream_host", None)
+            if self.stream_host is None:
+                self.stream_host = self.stream.cpu().numpy()
+            return self.stream_host
+        return self.stream
+
+    def host_chunk_off(self) -> np.ndarray:
+        return self.chunk_off if isinstance(self.chunk_off, np.ndarray) else self.chunk_off.cpu().numpy()
+
+    @property
+    def n_chunks(self) -> int:
+        return len(self.chunk_off)
+
+    @property
+    def n_stream(self) -> int:
+        return len(self.stream)
 
 
 def topic_tokens(n_tokens: int, vocab: int, topics: int, zipf_s: float, *, sentence_len: int = 1000,
@@ -278,8 +298,9 @@ def topic_corpus_gpu(n_tokens: int, vocab: int, topics: int, zipf_s: float, *, m
     vocab_of_raw[order] = torch.arange(1, len(order) + 1, device=dev)
     vid = vocab_of_raw[train_raw]
     ids = vid[vid >= 0].to(torch.int32)
-    stream = torch.cat([ids, torch.zeros(1, dtype=torch.int32, device=dev)]).cpu().numpy()
-    chunk_off = np.arange(0, len(ids), msl, dtype=np.int64)
+    # the stream and its chunks stay on the device (fw2v_load_corpus_device)
+    stream = torch.cat([ids, torch.zeros(1, dtype=torch.int32, device=dev)])
+    chunk_off = torch.arange(0, len(ids), msl, dtype=torch.int64, device=dev)
     counts_np = counts.cpu().numpy().astype(np.uint32)
     label = np.concatenate([[-1], planted[order].cpu().numpy()]).astype(np.int32)
     raw_of_vocab = np.concatenate([[-1], order.cpu().numpy()]).astype(np.int64)
@@ -289,7 +310,7 @@ def topic_corpus_gpu(n_tokens: int, vocab: int, topics: int, zipf_s: float, *, m
     if heldout_tokens:
         hv = vocab_of_raw[raw[n_tokens:].long()]
         held = hv[hv >= 0].to(torch.int32).cpu().numpy()
-    del raw, train_raw, vid, ids
+    del raw, train_raw, vid
     if dev.type == "cuda":
         torch.cuda.empty_cache()
     return corpus, held
@@ -310,16 +331,22 @@ def make_topic_corpus_gpu(name: str, *, n_tokens: int | None = None, heldout_tok
 
 def sbm_corpus_gpu(nodes: int, blocks: int, degree: float, p_ratio: float, walks_per_node: int, walk_len: int, *,
                    seed: int = 0, device="cuda", min_count: int = 1, heldout_walks: int = 0):
-    """sbm_walks() generated with torch on a device, written as the reference's
-    text front end would read the walks one per line with -cache-eos: every
-    walk is a sentence ending in </s> and a stored chunk of its own.  The
-    vocabulary is the visited nodes by count (ties by first occurrence).
+    """sbm_walks() generated on a device, written as the reference's text
+    front end would read the walks one per line with -cache-eos: every walk is
+    a sentence ending in </s> and a stored chunk of its own.  The graph is
+    built with torch; the walks come from this library's walk kernel
+    (fw2v_random_walks, counter-based per (seed, walk, step)) straight into the
+    token stream, which stays on the device.  The vocabulary is the visited
+    nodes by count (ties by first occurrence).
 
     Returns (SynthCorpus with each node's block as its label and purity 1,
     held-out walks as int32 vocab ids with a 0 after each, or None).
     """
     import torch
 
+    from . import lib
+    if min_count > 1:
+        raise ValueError("walk corpora keep every visited node (min_count 1)")
     dev = torch.device(device)
     gen = torch.Generator(device=device)
     gen.manual_seed(seed)
@@ -341,60 +368,57 @@ def sbm_corpus_gpu(nodes: int, blocks: int, degree: float, p_ratio: float, walks
     ok = src != dst
     src, dst = src[ok], dst[ok]
     order = torch.argsort(src, stable=True)
-    src, dst = src[order], dst[order]
+    src, dst = src[order], dst[order].to(torch.int32).contiguous()
     deg = torch.bincount(src, minlength=nodes)
     offs = torch.zeros(nodes + 1, device=dev, dtype=torch.int64)
     offs[1:] = torch.cumsum(deg, 0)
     del a, b, c, d, keep, ok, order, src
+    cs = torch.cuda.current_stream(dev)
 
-    def walk(starts):
-        out = torch.empty((len(starts), walk_len), device=dev, dtype=torch.int64)
-        cur = starts.clone()
-        out[:, 0] = cur
-        for t in range(1, walk_len):
-            dc = deg[cur]
-            pick = (torch.rand(len(cur), device=dev, generator=gen, dtype=torch.float64) * dc).long()
-            cur = torch.where(dc > 0, dst[offs[cur] + pick.clamp(max=(dc - 1).clamp(min=0))], cur)
-            out[:, t] = cur
+    def walks(starts, wseed):
+        """Walks from `starts` as a stream: walk w at w * (walk_len + 1), raw
+        node ids, a -1 after each walk, one trailing slot."""
+        out = torch.empty(len(starts) * (walk_len + 1) + 1, device=dev, dtype=torch.int32)
+        st = lib().fw2v_random_walks(offs.data_ptr(), dst.data_ptr(), nodes, starts.data_ptr(), len(starts),
+                                     walk_len, wseed, out.data_ptr(), cs.cuda_stream)
+        if st != 0:
+            raise RuntimeError(f"fw2v_random_walks failed: status {st}")
+        out[-1] = -1
         return out
 
-    starts = torch.arange(nodes, device=dev, dtype=torch.int64).repeat_interleave(walks_per_node)
-    walks = walk(starts)
-    flat = walks.reshape(-1)
+    starts = torch.arange(nodes, device=dev, dtype=torch.int32).repeat_interleave(walks_per_node).contiguous()
+    stream = walks(starts, seed)
+    n_walks = len(starts)
+    body = stream[:-1].view(n_walks, walk_len + 1)[:, :walk_len]
+    flat = body.reshape(-1).long()
     n = flat.numel()
     cnt = torch.bincount(flat, minlength=nodes)
     first = torch.full((nodes,), n, device=dev, dtype=torch.int64)
     first.scatter_reduce_(0, flat, torch.arange(n, device=dev, dtype=torch.int64), reduce="amin")
+    del flat
     seen = torch.nonzero(cnt).flatten()
     vorder = seen[torch.argsort(first[seen], stable=True)]
     vorder = vorder[torch.argsort(-cnt[vorder], stable=True)]
-    vorder = vorder[cnt[vorder] >= min_count]
-    vocab_of = torch.full((nodes,), -1, device=dev, dtype=torch.int64)
-    vocab_of[vorder] = torch.arange(1, len(vorder) + 1, device=dev)
-    n_walks = walks.shape[0]
+    vocab_of = torch.zeros(nodes, device=dev, dtype=torch.int32)
+    vocab_of[vorder] = torch.arange(1, len(vorder) + 1, device=dev, dtype=torch.int32)
     counts = torch.cat([torch.tensor([max(n_walks - 1, 0)], device=dev), cnt[vorder]]).cpu().numpy().astype(np.uint32)
 
-    def lines(w):
-        ids = vocab_of[w]
-        ids = torch.cat([ids, torch.zeros((w.shape[0], 1), device=dev, dtype=torch.int64)], 1)
-        ids = ids.reshape(-1)
-        return ids[ids >= 0].to(torch.int32)
+    def relabel(t):
+        st = lib().fw2v_relabel_stream(t.data_ptr(), t.numel(), vocab_of.data_ptr(), nodes, cs.cuda_stream)
+        if st != 0:
+            raise RuntimeError(f"fw2v_relabel_stream failed: status {st}")
+        return t
 
-    if min_count > 1:
-        raise ValueError("walk corpora keep every visited node (min_count 1)")
-    stream_t = lines(walks)
-    stream = torch.cat([stream_t, torch.zeros(1, device=dev, dtype=torch.int32)]).cpu().numpy()
-    chunk_off = np.arange(n_walks, dtype=np.int64) * (walk_len + 1)
+    relabel(stream)  # node ids -> vocabulary ids, the separators and the trailing slot -> 0
+    chunk_off = torch.arange(n_walks, device=dev, dtype=torch.int64) * (walk_len + 1)
     label = np.concatenate([[-1], block[vorder].cpu().numpy()]).astype(np.int32)
     raw_of_vocab = np.concatenate([[-1], vorder.cpu().numpy()]).astype(np.int64)
     purity = np.concatenate([[0.0], np.ones(len(vorder))])
     corpus = SynthCorpus(counts, int(counts.sum()) + 1, stream, chunk_off, label, raw_of_vocab, purity)
     held = None
     if heldout_walks:
-        hs = torch.randint(0, nodes, (heldout_walks,), device=dev, generator=gen)
-        hw = walk(hs)
-        held = lines(hw).cpu().numpy()
-    del walks, flat, stream_t
+        hs = torch.randint(0, nodes, (heldout_walks,), device=dev, generator=gen).to(torch.int32).contiguous()
+        held = relabel(walks(hs, seed ^ 0x48454C44))[:-1].cpu().numpy()
     if dev.type == "cuda":
         torch.cuda.empty_cache()
     return corpus, held
