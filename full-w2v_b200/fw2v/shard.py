@@ -18,3 +18,36 @@ def assign_jobs(tokens: list[int], n_ranks: int) -> list[list[int]]:
         out[r].append(j)
         load[r] += tokens[j]
     return [sorted(x) for x in out]
+
+
+def job_tokens(specs: list[dict]) -> list[int]:
+    """Tokens of each graph job (walks per node x nodes x (walk length + 1))."""
+    return [s["nodes"] * s["walks_per_node"] * (s["walk_len"] + 1) for s in specs]
+
+
+def rank_share(specs: list[dict], world: int, rank: int) -> list[int]:
+    """This rank's jobs (indices into specs) under assign_jobs."""
+    return assign_jobs(job_tokens(specs), world)[rank]
+
+
+def combine_ranks(words: float, seconds: float, alone_words: float = 0.0, alone_seconds: float = 0.0,
+                  device=None) -> dict:
+    """Whole-job figures of a partitioned batch: words summed over ranks, time
+    the slowest rank's (max), for the batch and for the jobs trained alone.
+    Uses torch.distributed when a process group is initialised (any backend;
+    `device` is where the reduction tensors live: "cuda" under NCCL, "cpu"
+    under gloo), else this process alone.  Every rank calls it at the same
+    point (two all-reduces, the same on every rank)."""
+    import torch
+    import torch.distributed as dist
+
+    w = torch.tensor([float(words), float(alone_words)], dtype=torch.float64, device=device)
+    t = torch.tensor([float(seconds), float(alone_seconds)], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized():
+        dist.all_reduce(w, op=dist.ReduceOp.SUM)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    w, t = w.cpu().tolist(), t.cpu().tolist()
+    out = {"words": w[0], "seconds": t[0], "value": w[0] / t[0] if t[0] > 0 else 0.0}
+    if t[1] > 0:
+        out.update(alone_words=w[1], alone_seconds=t[1], alone_value=w[1] / t[1])
+    return out
