@@ -14,10 +14,17 @@ Own arm (default): the library's epoch loop through its C ABI.
   e2e     the same through the public API from host buffers: every step copies
           the token stream from pinned host memory (fw2v_load_corpus), trains
           one epoch and reads the word count back.
-Reference arm (--impl reference): the reference's own program built from its
-sources for sm_100a (oracle/_ref/FULL-W2V) on the same corpus written as text,
-its host threads on all host cores; or, where it cannot run, the CPU
-restatement of its training path (oracle port).
+  reference_gpu  (N=1) the reference's own CUDA program (baseline/_ref/FULL-W2V,
+          built unmodified from its sources for sm_100a) and this project's
+          plain FP32 kernel, each training the text-scale corpus (C2) for its 5
+          epochs on this GPU: the reference's "Overall Words Per Second" beside
+          ours.  The reference kernel cannot run the default workload (d=300:
+          its 8-float reduce scratch overlaps index_cache for d > 256,
+          FULL-W2V-kernels.cu:117-120, and d % 32 != 0 gives partial-warp
+          shuffles).
+Reference arm (--impl reference): the reference's own program on the same
+corpus written as text (c1/c2), its host threads on all host cores; or, where
+it cannot run, the CPU restatement of its training path (oracle port).
 
 Multi-GPU (torchrun): replicas only — every rank trains its own copy of the job,
 value = words of all ranks / max over ranks of the timed device time.
@@ -166,7 +173,7 @@ def cpu_baseline(corpus, cfg, threads, seconds_target=15.0):
     cores = os.cpu_count() or 1
     d = cfg["d"]
     V = len(corpus.counts)
-    ocorp = O.Corpus(corpus.stream, corpus.chunk_off, corpus.counts, [], corpus.train_words)
+    ocorp = O.Corpus(corpus.host_stream(), corpus.host_chunk_off(), corpus.counts, [], corpus.train_words)
     kw = dict(threads=threads, msl=1000, negative=cfg["negative"], epochs=1, alpha0=0.025,
               sample=cfg["sample"], d=d, window=cfg["window"], n_threads=cores)
     syn0 = O.init_syn0(V, d, d)
@@ -322,7 +329,8 @@ def run_own(args, world, rank, local):
 
     # e2e: through the public API from pinned host buffers, every step
     pinned = torch.empty(len(corpus.stream), dtype=torch.int32, pin_memory=True)
-    pinned.numpy()[:] = corpus.stream
+    pinned.numpy()[:] = corpus.host_stream()
+    host_chunks = corpus.host_chunk_off()
     host_stream = pinned.numpy()
     e2e_steps = max(1, min(args.steps, 2))
     e2e_words, e2e_s = 0, 0.0
@@ -334,7 +342,7 @@ def run_own(args, world, rank, local):
         if form.endswith("batched"):
             with fw2v.Batch(precision=prec, device=local, group_bytes=args.group_bytes) as eb:
                 eb.add_job(job_config(args, cfg, T, 1, prec), corpus.counts, corpus.train_words, host_stream,
-                           corpus.chunk_off)
+                           host_chunks)
                 if args.shape:
                     eb.set_shape(0, *[int(x) for x in args.shape.split(",")])
                     if args.wpb:
@@ -347,13 +355,13 @@ def run_own(args, world, rank, local):
         else:
             with fw2v.Trainer(job_config(args, cfg, T, 1, prec)) as et:
                 et.set_vocab(corpus.counts, corpus.train_words)
-                et.load_corpus(host_stream, corpus.chunk_off)
+                et.load_corpus(host_stream, host_chunks)
                 et.sample_epoch()
                 e2e_words += et.train_sampled().words_read
         e2e_s += time.perf_counter() - t0
     e2e_s = max_over_ranks(world, e2e_s)
     e2e_value = sum_over_ranks(world, float(e2e_words)) / e2e_s
-    h2d = corpus.stream.nbytes + corpus.chunk_off.nbytes + corpus.counts.nbytes
+    h2d = 4 * len(corpus.stream) + 8 * len(corpus.chunk_off) + corpus.counts.nbytes
     d2h = 8 * T + 16
 
     # the plain FP32 kernel on the same workload, for the form's speed-up
@@ -444,9 +452,122 @@ def run_own(args, world, rank, local):
     clocks = clk.summary()
     if clocks:
         out["clocks"] = clocks
+    if args.config == "c3":
+        out["config"]["notes"] = (
+            "subsampling is inactive at this corpus shape (kept_fraction 1.0): the 1000-topic mixture flattens "
+            "every word's marginal frequency below the sample=1e-4 threshold; same-topic precision@10 after one "
+            "epoch is at chance for both precisions (about 1% of context pairs share a topic), so the held-out "
+            "SGNS loss is the quality gate here")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(corpus, cfg, T)
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        del corpus, held, pairs
+        out["reference_gpu"] = reference_gpu(local)
     return out
+
+
+def safe_reference_threads(corpus, cfg, epochs, cores, streams=4, batch=200):
+    """Host threads for the reference program under which every launch reads
+    only buffers it has filled: each thread must ship more than streams x
+    batch sentences over the run, or its final launch (FULL-W2V-driver.cu:
+    305-318, all `batch` blocks of stream S-1) replays unfilled buffers.
+    Sentences per thread come from this library's sampler, which reproduces
+    the reference's batch builder bit for bit."""
+    import fw2v
+    threads = min(cores, len(corpus.chunk_off))
+    while threads >= 1:
+        c = fw2v.default_config(layer_size=8, window=cfg["window"], negative=cfg["negative"], epochs=1,
+                                threads=threads, msl=1000, alpha=0.025, sample=cfg["sample"])
+        with fw2v.Trainer(c) as t:
+            t.set_vocab(corpus.counts, corpus.train_words)
+            t.load_corpus(corpus.stream, corpus.chunk_off)
+            t.sample_epoch()
+            least = min(len(r[0]) for r in t.epoch_samples())
+        if least * epochs >= streams * batch + 1:
+            return threads
+        threads //= 2
+    return 0
+
+
+def run_reference_program(binary, text, cfg, epochs, threads, streams=4, batch=200):
+    """FULL-W2V on a text corpus; (words/s, overall seconds) or a reason string."""
+    cmd = [binary, "-train", text, "-size", str(cfg["d"]), "-window", str(cfg["window"]),
+           "-negative", str(cfg["negative"]), "-sample", str(cfg["sample"]), "-iter", str(epochs),
+           "-alpha", "0.025", "-min-count", str(cfg["min_count"]), "-threads", str(threads),
+           "-streams", str(streams), "-kernel-batch-size", str(batch), "-msl", "1000",
+           "-debug", "0", "-no-export", "-output", os.devnull]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        return f"reference exited {r.returncode}: {r.stderr[-300:]}"
+    wps = [ln for ln in r.stdout.splitlines() if ln.startswith("Overall Words Per Second:")]
+    tim = [ln for ln in r.stdout.splitlines() if ln.startswith("Overall time:")]
+    if not wps:
+        return "no words/sec line from the reference"
+    return float(wps[0].split(":")[1]), (float(tim[0].split(":")[1]) if tim else None)
+
+
+def reference_gpu(local):
+    """The reference's CUDA program and the plain FP32 kernel of this library on
+    the same text-scale corpus (C2: 17M tokens, V=71k after min-count 5,
+    d=128, window 8, negative 5, sample 1e-4, 5 epochs), one after the other
+    on this GPU.  Each rate is the implementation's own: the reference's
+    "Overall Words Per Second" (its clock runs from after set-up to its final
+    device sync, FULL-W2V-driver.cu:162, 324, 450); ours, words read over the
+    device time of the 5 epochs (sampler and trainer, CUDA events)."""
+    import torch
+
+    import fw2v
+    from fw2v import synth
+    binary = os.path.join(ROOT, "baseline", "_ref", "FULL-W2V")
+    if not os.path.exists(binary):
+        return {"unavailable": "baseline/_ref/FULL-W2V not built (make -C baseline with the reference checkout)"}
+    cfg = dict(synth.CONFIGS["c2"])
+    epochs = cfg["epochs"]
+    raw, planted, _ = synth.topic_tokens(cfg["n_tokens"], cfg["vocab"], cfg["topics"], cfg["zipf_s"], seed=1236)
+    ends = np.arange(1000, len(raw) + 1000, 1000)
+    ends[-1] = len(raw)
+    corpus = synth.build_stream(raw, ends, planted, min_count=cfg["min_count"], msl=1000)
+    cores = os.cpu_count() or 1
+    threads = safe_reference_threads(corpus, cfg, epochs, cores)
+    if threads < 1:
+        return {"unavailable": "corpus too small for the reference's launch pattern"}
+    tmp = tempfile.mkdtemp(prefix="fw2v_ref_")
+    try:
+        text = os.path.join(tmp, "corpus.txt")
+        with open(text, "wb") as f:
+            f.write(synth.text_of(raw, ends))
+        del raw
+        ref = run_reference_program(binary, text, cfg, epochs, threads)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    if isinstance(ref, str):
+        return {"unavailable": ref}
+    dev = torch.device("cuda", local)
+    T = default_streams(len(corpus.chunk_off))
+    c = fw2v.default_config(layer_size=cfg["d"], window=cfg["window"], negative=cfg["negative"], epochs=epochs,
+                            threads=T, msl=1000, alpha=0.025, sample=cfg["sample"])
+    with fw2v.Trainer(c) as t:
+        t.set_vocab(corpus.counts, corpus.train_words)
+        t.load_corpus(corpus.stream, corpus.chunk_off)
+        ts = torch.cuda.ExternalStream(t.stream_handle(), device=dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(ts)
+        words = t.train()
+        e1.record(ts)
+        e1.synchronize()
+        secs = e0.elapsed_time(e1) / 1e3
+    ours = words / secs
+    return {"workload": f"c2: {cfg['n_tokens'] / 1e6:.0f}M-token topic corpus, V={len(corpus.counts)}, d={cfg['d']}, "
+                        f"window={cfg['window']}, negative={cfg['negative']}, sample={cfg['sample']}, msl=1000, "
+                        f"{epochs} epochs; both on this GPU, one after the other",
+            "reference": {"value": ref[0], "unit": UNIT, "overall_time_s": ref[1], "host_threads": threads,
+                          "streams": 4, "kernel_batch_size": 200,
+                          "program": "baseline/_ref/FULL-W2V: the reference's FULL-W2V-driver.cu and "
+                                     "FULL-W2V-kernels.cu, unmodified, nvcc -O3 -Xptxas -dlcm=ca for sm_100a"},
+            "fp32_plain": {"value": ours, "unit": UNIT, "device_time_s": secs, "words": int(words),
+                           "sampling_streams": T, "kernel": "sgns_train_kernel, default shape"},
+            "speedup": ours / ref[0]}
 
 
 def run_c5(args, world, rank, local):
@@ -462,13 +583,12 @@ def run_c5(args, world, rank, local):
 
     import fw2v
     from fw2v import evaluate, synth
-    from fw2v.shard import assign_jobs
+    from fw2v.shard import combine_ranks, rank_share
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     all_specs = synth.c5_job_specs(scale=args.scale)
-    tokens = [s["nodes"] * s["walks_per_node"] * (s["walk_len"] + 1) for s in all_specs]
-    specs = [all_specs[j] for j in assign_jobs(tokens, world)[rank]]
+    specs = [all_specs[j] for j in rank_share(all_specs, world, rank)]
     prec = fw2v.BF16 if args.form.startswith("bf16") else fw2v.FP32
     batch = fw2v.Batch(precision=prec, device=local, group_bytes=args.group_bytes)
     labels, alone_p10, alone_ms, alone_words = [], [], 0.0, 0
@@ -501,9 +621,8 @@ def run_c5(args, world, rank, local):
         st = batch.train()
         torch.cuda.synchronize(dev)
     barrier(world)
-    batch_s = max_over_ranks(world, st.ms / 1e3)
-    words_all = sum_over_ranks(world, float(st.words_read))
-    value = words_all / batch_s
+    tot = combine_ranks(st.words_read, st.ms / 1e3, alone_words, alone_ms / 1e3, device=dev)
+    batch_s, words_all, value = tot["seconds"], tot["words"], tot["value"]
     p10 = [evaluate.precision_at_10(batch.syn0(j), *labels[j][:2], purity=labels[j][2], device=dev)[0]
            for j in range(len(specs))]
     batch.close()
@@ -521,7 +640,7 @@ def run_c5(args, world, rank, local):
            "gpu_launches": 5 * st.rounds}
     if alone_p10:
         diff = np.array(p10) - np.array(alone_p10)
-        alone_value = sum_over_ranks(world, float(alone_words)) / max_over_ranks(world, alone_ms / 1e3)
+        alone_value = tot["alone_value"]
         out["fp32_alone"] = {"form": "each job alone, fp32 single-job kernel", "value": alone_value,
                              "unit": UNIT, "speedup": value / alone_value,
                              "precision_at_10_mean": float(np.nanmean(alone_p10)),
@@ -547,14 +666,14 @@ def run_reference(args, world, rank):
     corpus, _, cfg = make_corpus(args)
     T_stream = args.streams or default_streams(len(corpus.chunk_off))
     cores = os.cpu_count() or 1
-    binary = os.path.join(ROOT, "oracle", "_ref", "FULL-W2V")
+    binary = os.path.join(ROOT, "baseline", "_ref", "FULL-W2V")
     reason = None
     if args.config not in ("c1", "c2"):
         reason = f"{args.config} is generated on the device and is not written as text for the reference program"
     elif cfg["d"] > 256 or cfg["d"] % 32:
         reason = f"reference kernel unsupported at d={cfg['d']} (shared-memory overlap / partial warp)"
     elif not os.path.exists(binary):
-        reason = "oracle/_ref/FULL-W2V not built"
+        reason = "baseline/_ref/FULL-W2V not built"
     if reason is None:
         res = reference_program(args, corpus, cfg, binary, cores)
         if isinstance(res, dict):
@@ -572,54 +691,29 @@ def run_reference(args, world, rank):
 
 
 def reference_program(args, corpus, cfg, binary, cores):
-    """Run FULL-W2V with thread/stream/batch settings under which every launch
-    reads only buffers it has filled: each host thread must complete >= S full
-    batches before its final launch (FULL-W2V-driver.cu:305-318 launches all
-    kernel-batch-size blocks and reuses the buffers of stream S-1 otherwise
-    unfilled).  Sentence counts per thread come from the oracle's restatement of
-    the reference batch builder."""
-    from fw2v import synth
-    from oracle import oracle as O
-
+    """FULL-W2V on the workload's corpus written as text, with host threads
+    under which every launch reads only buffers it has filled
+    (safe_reference_threads)."""
+    epochs = args.steps
+    threads = safe_reference_threads(corpus, cfg, epochs, cores)
+    if threads < 1:
+        return "corpus too small for the reference's launch pattern"
     raw_text = synth_text(args, cfg)
     if raw_text is None:
         return "could not write the corpus as text"
-    epochs = args.steps
-    batch, streams = 200, 4
-    ocorp = O.Corpus(corpus.stream, corpus.chunk_off, corpus.counts, [], corpus.train_words)
-    threads = min(cores, len(corpus.chunk_off))
-    while threads >= 1:
-        per = O.sample_streams(ocorp, threads=threads, msl=1000, negative=cfg["negative"],
-                               epochs=1, alpha0=0.025, sample=cfg["sample"])
-        min_entries = min(len(p[0].lens) for p in per) * epochs
-        if min_entries >= streams * batch + 1:
-            break
-        threads //= 2
-    if threads < 1:
-        return "corpus too small for the reference's launch pattern"
-    cmd = [binary, "-train", raw_text, "-size", str(cfg["d"]), "-window", str(cfg["window"]),
-           "-negative", str(cfg["negative"]), "-sample", str(cfg["sample"]), "-iter", str(epochs),
-           "-alpha", "0.025", "-min-count", str(cfg["min_count"]), "-threads", str(threads),
-           "-streams", str(streams), "-kernel-batch-size", str(batch), "-msl", "1000",
-           "-debug", "0", "-no-export", "-output", os.devnull]
     try:
-        r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+        res = run_reference_program(binary, raw_text, cfg, epochs, threads)
     finally:
         shutil.rmtree(os.path.dirname(raw_text), ignore_errors=True)
-    if r.returncode != 0:
-        return f"reference exited {r.returncode}: {r.stderr[-300:]}"
-    wps = [ln for ln in r.stdout.splitlines() if ln.startswith("Overall Words Per Second:")]
-    tim = [ln for ln in r.stdout.splitlines() if ln.startswith("Overall time:")]
-    if not wps:
-        return "no words/sec line from the reference"
-    value = float(wps[0].split(":")[1])
-    secs = float(tim[0].split(":")[1]) if tim else None
+    if isinstance(res, str):
+        return res
+    value, secs = res
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": epochs,
             "warmup": 0, "ms_per_step": secs * 1e3 / epochs if secs else None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (same seeded corpus, written as text)", "impl": "reference",
             "config": {"workload": f"{args.config} as text, reference FULL-W2V sm_100a",
-                       "threads": threads, "streams": streams, "kernel_batch_size": batch},
+                       "threads": threads, "streams": 4, "kernel_batch_size": 200},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": f"{epochs} epochs of the full corpus; the reference's "
                                        f"host threads on {threads} cores feed its sm_100a kernel"},
@@ -663,6 +757,8 @@ def main():
     ap.add_argument("--group-bytes", type=int, default=0,
                     help="batched forms: table bytes per group of interleaved jobs (0: half of L2, -1: one group)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's CUDA program against the plain FP32 kernel (C2)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":

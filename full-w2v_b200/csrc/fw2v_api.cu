@@ -26,6 +26,8 @@ cudaError_t launch_init_tables(void* syn0, bool bf16, int64_t V, int d, int64_t 
 size_t train_smem_bytes(int window, int64_t pitch, int warps, int r, bool prefetch, int elem);
 int64_t train_scratch_warps(int num_sms);
 cudaError_t launch_validate_ids(const int32_t* ids, int64_t n, int64_t vocab, int* flag, cudaStream_t st);
+cudaError_t launch_check_corpus(const int32_t* stream, int64_t len, const int64_t* chunk_off, int64_t n, int* flag,
+                                cudaStream_t st);
 cudaError_t launch_corpus_layout(const int32_t* stream, int64_t stream_len, const int64_t* chunk_off,
                                  int64_t n_chunks, int msl, int threads, int64_t* chunk_base,
                                  int64_t* stream_base, cudaStream_t st);
@@ -385,15 +387,33 @@ static fw2v_status check_chunks(fw2v_handle* h, const int64_t* chunk_off, int64_
   return FW2V_OK;
 }
 
-fw2v_status fw2v_load_corpus(fw2v_handle* h, const int32_t* stream, int64_t stream_len, const int64_t* chunk_off,
-                             int64_t n_chunks) {
+// The corpus from host memory (on_device false: checked here, copied host to
+// device) or from device memory (checked by a kernel, copied on the device).
+static fw2v_status load_corpus(fw2v_handle* h, const int32_t* stream, int64_t stream_len, const int64_t* chunk_off,
+                               int64_t n_chunks, bool on_device) {
   if (!h || !stream || !chunk_off || stream_len < 1 || n_chunks < 1)
     return fail(h, FW2V_ERR_ARGUMENT, "load_corpus: empty corpus");
   if (h->V == 0) return fail(h, FW2V_ERR_STATE, "load_corpus before set_vocab");
-  if (stream[stream_len - 1] != 0) return fail(h, FW2V_ERR_ARGUMENT, "load_corpus: stream must end with 0");
-  fw2v_status s = check_chunks(h, chunk_off, n_chunks, stream_len);
-  if (s != FW2V_OK) return s;
+  fw2v_status s = FW2V_OK;
+  if (!on_device) {
+    if (stream[stream_len - 1] != 0) return fail(h, FW2V_ERR_ARGUMENT, "load_corpus: stream must end with 0");
+    s = check_chunks(h, chunk_off, n_chunks, stream_len);
+    if (s != FW2V_OK) return s;
+  } else if (h->cfg.threads > n_chunks || h->cfg.threads > 65535) {
+    return fail(h, FW2V_ERR_ARGUMENT, "threads (%d) > sentence chunks (%lld)", h->cfg.threads, (long long)n_chunks);
+  }
   CK(h, cudaSetDevice(h->cfg.device));
+  if (on_device) {
+    CK(h, launch_check_corpus(stream, stream_len, chunk_off, n_chunks, h->error_flag, h->stream));
+    int flag = 0;
+    CK(h, cudaMemcpyAsync(&flag, h->error_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (flag) {
+      CK(h, cudaMemsetAsync(h->error_flag, 0, sizeof(int), h->stream));
+      return fail(h, FW2V_ERR_ARGUMENT, "load_corpus_device: the stream must end with 0 and every chunk start in it");
+    }
+  }
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   const int T = h->cfg.threads;
   // Nothing may still read the previous corpus.
   CK(h, cudaStreamSynchronize(h->sstream));
@@ -417,8 +437,8 @@ fw2v_status fw2v_load_corpus(fw2v_handle* h, const int32_t* stream, int64_t stre
   }
   h->stream_len = stream_len;
   h->n_chunks = n_chunks;
-  CK(h, cudaMemcpyAsync(h->stream_ids, stream, stream_len * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
-  CK(h, cudaMemcpyAsync(h->chunk_off, chunk_off, n_chunks * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(h->stream_ids, stream, stream_len * sizeof(int32_t), kind, h->stream));
+  CK(h, cudaMemcpyAsync(h->chunk_off, chunk_off, n_chunks * sizeof(int64_t), kind, h->stream));
   CK(h, launch_validate_ids(h->stream_ids, stream_len, h->V, h->error_flag, h->stream));
   s = layout_streams(h);
   if (s != FW2V_OK) return s;
@@ -435,6 +455,16 @@ fw2v_status fw2v_load_corpus(fw2v_handle* h, const int32_t* stream, int64_t stre
   h->epochs_done = 0;
   h->words_total = 0;
   return FW2V_OK;
+}
+
+fw2v_status fw2v_load_corpus(fw2v_handle* h, const int32_t* stream, int64_t stream_len, const int64_t* chunk_off,
+                             int64_t n_chunks) {
+  return load_corpus(h, stream, stream_len, chunk_off, n_chunks, false);
+}
+
+fw2v_status fw2v_load_corpus_device(fw2v_handle* h, const int32_t* stream, int64_t stream_len,
+                                    const int64_t* chunk_off, int64_t n_chunks) {
+  return load_corpus(h, stream, stream_len, chunk_off, n_chunks, true);
 }
 
 fw2v_status fw2v_reorder_chunks(fw2v_handle* h, const int64_t* chunk_off, int64_t n_chunks) {

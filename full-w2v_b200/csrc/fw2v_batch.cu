@@ -33,6 +33,8 @@ cudaError_t launch_init_tables(void* syn0, bool bf16, int64_t V, int d, int64_t 
                                int n_firsts, int32_t* unigram, int64_t table_size, uint64_t start,
                                cudaStream_t st);
 cudaError_t launch_validate_ids(const int32_t* ids, int64_t n, int64_t vocab, int* flag, cudaStream_t st);
+cudaError_t launch_check_corpus(const int32_t* stream, int64_t len, const int64_t* chunk_off, int64_t n, int* flag,
+                                cudaStream_t st);
 cudaError_t launch_corpus_layout(const int32_t* stream, int64_t stream_len, const int64_t* chunk_off,
                                  int64_t n_chunks, int msl, int threads, int64_t* chunk_base,
                                  int64_t* stream_base, cudaStream_t st);
@@ -180,17 +182,7 @@ struct fw2v_batch {
   int64_t scratch_elems = 0, scratch_warps = 0, scratch_bytes = 0;
   int warps_per_block[kBatchFamilies] = {4, 4, 4}, blocks_per_sm[kBatchFamilies] = {0, 0, 0};  // per family
   int epochs_run = 0;  // batch epochs trained so far: job j has trained min(epochs_run, its epochs)
-  // The first round of the next epoch may already be sampled (by the end of
-  // the previous train call, while the host returns) into buf[next_buf];
-  // pre_* hold the state from before that sampling, to undo it.
-  int next_buf = 0;
-  bool presampled = false;
-  uint64_t* pre_lcg = nullptr;
-  uint64_t* pre_wca = nullptr;
-  float* pre_alpha = nullptr;
-  int64_t* pre_uid = nullptr;
-  unsigned long long* pre_words = nullptr;
-  unsigned long long* pre_kept = nullptr;
+  int next_buf = 0;  // the buffer set of the next round
   std::vector<unsigned long long> words_snap, kept_snap;  // counters at the end of the last call
   std::vector<cudaEvent_t> round_ev;  // 2 per training launch of a call: its device time
 };
@@ -330,8 +322,6 @@ TrainParams train_params(const fw2v_batch* b, const BatchJob& j, const RoundBuf&
   return p;
 }
 
-fw2v_status cancel_presample(fw2v_batch* b);
-
 // Streams of the jobs with in[j] set, in training order.  Jobs, in index
 // order, are gathered into groups whose tables together fit the group budget
 // (a larger job is a group of its own); a group's streams are taken
@@ -372,8 +362,6 @@ std::vector<StreamItem> stream_order(const fw2v_batch* b, const std::vector<char
 fw2v_status plan(fw2v_batch* b) {
   if (b->planned) return FW2V_OK;
   if (b->jobs.empty()) return bfail(b, FW2V_ERR_STATE, "batch has no jobs");
-  const fw2v_status pre = cancel_presample(b);  // its round and buffer are about to go
-  if (pre != FW2V_OK) return pre;
   free_plan(b);
   const int64_t cap = b->cfg.round_tokens > 0 ? b->cfg.round_tokens : (int64_t)1 << 27;
   for (int fam = 0; fam < kBatchFamilies; fam++) {
@@ -544,19 +532,14 @@ cudaError_t enqueue_epochs(fw2v_batch* b, int e0, int epochs, const Grid* grids,
   if (e == cudaSuccess) e = cudaStreamWaitEvent(b->sst, b->ev_fork, 0);
   int64_t k = 0;
   for (int ep = e0; ep < e0 + epochs && e == cudaSuccess; ep++) {
-    // the first round sampled ahead: its sampling (and the training stream's
-    // wait for it) happened before this sequence
-    const bool ahead = ep == e0 && b->presampled;
-    if (!ahead) e = cudaMemsetAsync(b->job_uid, 0, b->jobs.size() * sizeof(int64_t), b->sst);
+    e = cudaMemsetAsync(b->job_uid, 0, b->jobs.size() * sizeof(int64_t), b->sst);
     for (size_t ri = 0; ri < b->rounds.size() && e == cudaSuccess; ri++, k++) {
       RoundBuf& rb = b->buf[(b->next_buf + k) % 2];
       const RoundPlan& r = b->rounds[ri];
-      if (!(ahead && ri == 0)) {
-        if (k >= 2) e = cudaStreamWaitEvent(b->sst, rb.freed, 0);
-        if (e == cudaSuccess) e = enqueue_sample(b, rb, r.view, r.max_region, ep);
-        if (e == cudaSuccess) e = cudaEventRecord(rb.ready, b->sst);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->st, rb.ready, 0);
-      }
+      if (k >= 2 && e == cudaSuccess) e = cudaStreamWaitEvent(b->sst, rb.freed, 0);
+      if (e == cudaSuccess) e = enqueue_sample(b, rb, r.view, r.max_region, ep);
+      if (e == cudaSuccess) e = cudaEventRecord(rb.ready, b->sst);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(b->st, rb.ready, 0);
       if (e == cudaSuccess) e = cudaMemsetAsync(b->counter, 0, sizeof(unsigned long long), b->st);
       const Grid& g = grids[r.family];
       if (e == cudaSuccess) e = cudaEventRecordWithFlags(b->round_ev[2 * k], b->st, ev_flags);
@@ -568,50 +551,6 @@ cudaError_t enqueue_epochs(fw2v_batch* b, int e0, int epochs, const Grid* grids,
   if (e == cudaSuccess) e = cudaEventRecord(b->ev_join, b->sst);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(b->st, b->ev_join, 0);
   return e;
-}
-
-// Sample the first round of epoch `ep` into buf[next_buf] on the sampler
-// stream (not waited for), keeping the state it changes to undo it.
-fw2v_status presample(fw2v_batch* b, int ep) {
-  const size_t J = b->jobs.size();
-  const int64_t G = b->n_gstreams;
-  if (!b->pre_lcg) {
-    BCK(b, balloc(b->pre_lcg, G));
-    BCK(b, balloc(b->pre_wca, G));
-    BCK(b, balloc(b->pre_alpha, G));
-    BCK(b, balloc(b->pre_uid, J));
-    BCK(b, balloc(b->pre_words, J));
-    BCK(b, balloc(b->pre_kept, J));
-  }
-  BCK(b, cudaMemcpyAsync(b->pre_lcg, b->lcg, G * 8, cudaMemcpyDeviceToDevice, b->sst));
-  BCK(b, cudaMemcpyAsync(b->pre_wca, b->wca, G * 8, cudaMemcpyDeviceToDevice, b->sst));
-  BCK(b, cudaMemcpyAsync(b->pre_alpha, b->alpha, G * 4, cudaMemcpyDeviceToDevice, b->sst));
-  BCK(b, cudaMemcpyAsync(b->pre_uid, b->job_uid, J * 8, cudaMemcpyDeviceToDevice, b->sst));
-  BCK(b, cudaMemcpyAsync(b->pre_words, b->job_words, J * 8, cudaMemcpyDeviceToDevice, b->sst));
-  BCK(b, cudaMemcpyAsync(b->pre_kept, b->job_kept, J * 8, cudaMemcpyDeviceToDevice, b->sst));
-  RoundBuf& rb = b->buf[b->next_buf];
-  const RoundPlan& r = b->rounds[0];
-  BCK(b, cudaMemsetAsync(b->job_uid, 0, J * sizeof(int64_t), b->sst));
-  BCK(b, enqueue_sample(b, rb, r.view, r.max_region, ep));
-  BCK(b, cudaEventRecord(rb.ready, b->sst));
-  b->presampled = true;
-  return FW2V_OK;
-}
-
-// Undo a sampling ahead (before the jobs, the plan or buf[0] change).
-fw2v_status cancel_presample(fw2v_batch* b) {
-  if (!b->presampled) return FW2V_OK;
-  const size_t J = b->jobs.size();
-  const int64_t G = b->n_gstreams;
-  BCK(b, cudaStreamSynchronize(b->sst));
-  BCK(b, cudaMemcpy(b->lcg, b->pre_lcg, G * 8, cudaMemcpyDeviceToDevice));
-  BCK(b, cudaMemcpy(b->wca, b->pre_wca, G * 8, cudaMemcpyDeviceToDevice));
-  BCK(b, cudaMemcpy(b->alpha, b->pre_alpha, G * 4, cudaMemcpyDeviceToDevice));
-  BCK(b, cudaMemcpy(b->job_uid, b->pre_uid, J * 8, cudaMemcpyDeviceToDevice));
-  BCK(b, cudaMemcpy(b->job_words, b->pre_words, J * 8, cudaMemcpyDeviceToDevice));
-  BCK(b, cudaMemcpy(b->job_kept, b->pre_kept, J * 8, cudaMemcpyDeviceToDevice));
-  b->presampled = false;
-  return FW2V_OK;
 }
 
 fw2v_status check_error_flag(fw2v_batch* b, const char* what) {
@@ -707,8 +646,6 @@ void fw2v_batch_destroy(fw2v_batch* b) {
   bfree(b->jump_a); bfree(b->jump_c); bfree(b->exp_table); bfree(b->error_flag); bfree(b->counter);
   bfree(b->lcg); bfree(b->wca); bfree(b->alpha);
   bfree(b->job_uid); bfree(b->job_words); bfree(b->job_kept); bfree(b->orig_scratch);
-  bfree(b->pre_lcg); bfree(b->pre_wca); bfree(b->pre_alpha); bfree(b->pre_uid); bfree(b->pre_words);
-  bfree(b->pre_kept);
   for (RoundBuf& rb : b->buf)
     for (cudaEvent_t e : {rb.ready, rb.freed})
       if (e) cudaEventDestroy(e);
@@ -720,9 +657,27 @@ void fw2v_batch_destroy(fw2v_batch* b) {
   delete b;
 }
 
+static fw2v_status add_job(fw2v_batch* b, const fw2v_config* cfg, const uint32_t* counts, int64_t V,
+                           uint64_t train_words, const int32_t* stream, int64_t stream_len, const int64_t* chunk_off,
+                           int64_t n_chunks, int32_t* job_out, bool on_device);
+
 fw2v_status fw2v_batch_add_job(fw2v_batch* b, const fw2v_config* cfg, const uint32_t* counts, int64_t V,
                                uint64_t train_words, const int32_t* stream, int64_t stream_len,
                                const int64_t* chunk_off, int64_t n_chunks, int32_t* job_out) {
+  return add_job(b, cfg, counts, V, train_words, stream, stream_len, chunk_off, n_chunks, job_out, false);
+}
+
+fw2v_status fw2v_batch_add_job_device(fw2v_batch* b, const fw2v_config* cfg, const uint32_t* counts, int64_t V,
+                                      uint64_t train_words, const int32_t* stream, int64_t stream_len,
+                                      const int64_t* chunk_off, int64_t n_chunks, int32_t* job_out) {
+  return add_job(b, cfg, counts, V, train_words, stream, stream_len, chunk_off, n_chunks, job_out, true);
+}
+
+// A job from host memory (on_device false: the corpus checked here, copied
+// host to device) or device memory (checked by a kernel, copied on the device).
+static fw2v_status add_job(fw2v_batch* b, const fw2v_config* cfg, const uint32_t* counts, int64_t V,
+                           uint64_t train_words, const int32_t* stream, int64_t stream_len, const int64_t* chunk_off,
+                           int64_t n_chunks, int32_t* job_out, bool on_device) {
   if (!b || !cfg || !counts || !stream || !chunk_off) return bfail(b, FW2V_ERR_ARGUMENT, "null argument");
   const fw2v_config& c = *cfg;
   if (c.layer_size < 1 || c.layer_size > 384 || c.window < 1 || c.window > kMaxWindow || c.negative < 0 ||
@@ -733,14 +688,25 @@ fw2v_status fw2v_batch_add_job(fw2v_batch* b, const fw2v_config* cfg, const uint
   if (b->negative >= 0 && c.negative != b->negative)
     return bfail(b, FW2V_ERR_ARGUMENT, "batch job: negative %d differs from the batch's %d", c.negative, b->negative);
   if (V < 2 || V > (int64_t)INT32_MAX) return bfail(b, FW2V_ERR_ARGUMENT, "batch job: V >= 2 required");
-  if (stream_len < 1 || stream[stream_len - 1] != 0 || n_chunks < 1 || c.threads > n_chunks || c.threads > 65535)
+  if (stream_len < 1 || (!on_device && stream[stream_len - 1] != 0) || n_chunks < 1 || c.threads > n_chunks ||
+      c.threads > 65535)
     return bfail(b, FW2V_ERR_ARGUMENT, "batch job: stream must end with 0, threads <= chunks");
-  for (int64_t i = 0; i < n_chunks; i++)
-    if (chunk_off[i] < 0 || chunk_off[i] >= stream_len)
-      return bfail(b, FW2V_ERR_ARGUMENT, "batch job: chunk %lld starts outside the stream", (long long)i);
+  if (!on_device)
+    for (int64_t i = 0; i < n_chunks; i++)
+      if (chunk_off[i] < 0 || chunk_off[i] >= stream_len)
+        return bfail(b, FW2V_ERR_ARGUMENT, "batch job: chunk %lld starts outside the stream", (long long)i);
   BCK(b, cudaSetDevice(b->cfg.device));
-  fw2v_status pre = cancel_presample(b);
-  if (pre != FW2V_OK) return pre;
+  if (on_device) {
+    BCK(b, launch_check_corpus(stream, stream_len, chunk_off, n_chunks, b->error_flag, b->st));
+    int flag = 0;
+    BCK(b, cudaMemcpyAsync(&flag, b->error_flag, sizeof(int), cudaMemcpyDeviceToHost, b->st));
+    BCK(b, cudaStreamSynchronize(b->st));
+    if (flag) {
+      BCK(b, cudaMemsetAsync(b->error_flag, 0, sizeof(int), b->st));
+      return bfail(b, FW2V_ERR_ARGUMENT, "batch job: the stream must end with 0 and every chunk start in it");
+    }
+  }
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   BCK(b, cudaStreamSynchronize(b->st));
   BCK(b, cudaStreamSynchronize(b->sst));
   BatchJob j;
@@ -783,8 +749,8 @@ fw2v_status fw2v_batch_add_job(fw2v_batch* b, const fw2v_config* cfg, const uint
   step(cudaMemsetAsync(j.syn1neg, 0, tbytes, b->st));
   step(cudaMemcpyAsync(d_counts, counts, V * sizeof(uint32_t), cudaMemcpyHostToDevice, b->st));
   step(cudaMemcpyAsync(j.firsts, firsts.data(), (V - 1) * sizeof(int64_t), cudaMemcpyHostToDevice, b->st));
-  step(cudaMemcpyAsync(j.stream, stream, stream_len * sizeof(int32_t), cudaMemcpyHostToDevice, b->st));
-  step(cudaMemcpyAsync(j.chunk_off, chunk_off, n_chunks * sizeof(int64_t), cudaMemcpyHostToDevice, b->st));
+  step(cudaMemcpyAsync(j.stream, stream, stream_len * sizeof(int32_t), kind, b->st));
+  step(cudaMemcpyAsync(j.chunk_off, chunk_off, n_chunks * sizeof(int64_t), kind, b->st));
   if (e == cudaSuccess)
     step(launch_init_tables(j.syn0, b->elem == 2, V, c.layer_size, j.pitch, d_counts, c.sample, train_words,
                             j.keep_thr, nullptr, 0, nullptr, kUnigramTableSize, 1ULL + j.soff, b->st));
@@ -852,13 +818,6 @@ fw2v_status fw2v_batch_add_job(fw2v_batch* b, const fw2v_config* cfg, const uint
   b->kept_total.push_back(0);
   b->words_snap.push_back(0);
   b->kept_snap.push_back(0);
-  // the undo snapshots are sized by the stream and job counts: reallocated on use
-  bfree(b->pre_lcg);
-  bfree(b->pre_wca);
-  bfree(b->pre_alpha);
-  bfree(b->pre_uid);
-  bfree(b->pre_words);
-  bfree(b->pre_kept);
   b->planned = false;
   if (job_out) *job_out = (int32_t)b->jobs.size() - 1;
   return FW2V_OK;
@@ -938,7 +897,6 @@ fw2v_status fw2v_batch_train_epochs(fw2v_batch* b, int32_t n_epochs, fw2v_batch_
   }
   BCK(b, cudaStreamSynchronize(b->st));
   BCK(b, cudaEventRecord(b->ev_start, b->st));
-  if (b->presampled) BCK(b, cudaStreamWaitEvent(b->st, b->buf[b->next_buf].ready, 0));
   if (b->cfg.use_graph) {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -959,7 +917,6 @@ fw2v_status fw2v_batch_train_epochs(fw2v_batch* b, int32_t n_epochs, fw2v_batch_
     BCK(b, cudaEventRecord(b->ev_end, b->st));
     BCK(b, cudaStreamSynchronize(b->st));
   }
-  b->presampled = false;
   b->next_buf = (int)((b->next_buf + (int64_t)epochs * (int64_t)b->rounds.size()) % 2);
   s = check_error_flag(b, "batch train");
   if (s != FW2V_OK) return s;
@@ -988,10 +945,6 @@ fw2v_status fw2v_batch_train_epochs(fw2v_batch* b, int32_t n_epochs, fw2v_batch_
     out.train_ms += t;
   }
   out.train_launches = (int32_t)launches;
-  if (b->epochs_run < max_epochs) {  // the next call's first round, while the host returns
-    s = presample(b, b->epochs_run);
-    if (s != FW2V_OK) return s;
-  }
   out.epochs = epochs;
   out.rounds = (int32_t)b->rounds.size();
   if (stats) *stats = out;
@@ -1069,9 +1022,7 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
   if (!b) return FW2V_ERR_ARGUMENT;
   if (b->cfg.deterministic) return bfail(b, FW2V_ERR_STATE, "tuning needs the concurrent mode");
   BCK(b, cudaSetDevice(b->cfg.device));
-  fw2v_status s = cancel_presample(b);
-  if (s != FW2V_OK) return s;
-  s = plan(b);
+  fw2v_status s = plan(b);
   if (s != FW2V_OK) return s;
   if (sample_tokens <= 0) sample_tokens = (int64_t)1 << 23;
   const size_t J = b->jobs.size();

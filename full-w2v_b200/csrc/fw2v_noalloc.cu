@@ -1,9 +1,11 @@
 // fw2v_kernel_batch_noalloc: the kernel seam (fw2v_kernel_batch) for callers
-// that cannot allocate device memory — code recording a CUDA graph, where
-// cudaMalloc and cudaFree are not allowed; programs whose device memory belongs
-// to a framework's pool; loops that cannot afford an allocator call.  It runs
-// the same training kernel; the only difference is where the per-warp scratch
-// comes from: a fixed array in this file instead of a per-launch allocation.
+// that cannot allocate device memory — programs whose device memory belongs to
+// a framework's pool allocator (a direct cudaMalloc bypasses its accounting
+// and can fail once the pool holds the device), plugin hosts with a fixed
+// memory budget, and loops in which an allocator call would stall or
+// synchronise the device.  It runs the same training kernel; the only
+// difference is where the per-warp scratch comes from: a fixed array in this
+// file instead of a per-launch allocation.
 #include <mutex>
 
 #include "../../include/fw2v.h"
@@ -11,6 +13,7 @@
 
 namespace fw2v {
 cudaError_t launch_train(const TrainParams& p, int num_sms, cudaStream_t st);
+bool launch_fits(const TrainParams& p);
 fw2v_status seam_state(int dev, int** error_word, const float** exp_table, int* sms);
 }  // namespace fw2v
 
@@ -54,9 +57,16 @@ extern "C" fw2v_status fw2v_kernel_batch_noalloc(float* syn0, float* syn1neg, co
   const uint64_t warp_floats = (uint64_t)(2 * window + 1) * pitch;
   const uint64_t cap_warps = (FW2V_NOALLOC_SCRATCH_BYTES / sizeof(float)) / warp_floats;
   if (cap_warps < (uint64_t)fw2v::kWarpsPerBlock) return FW2V_ERR_TOO_LARGE;
-  if (n_blocks == 0) return FW2V_OK;
+  fw2v::TrainParams p{};
+  p.pitch = pitch;
+  p.d = layer_size;
+  p.window = window;
+  p.negative = negative;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return FW2V_ERR_NO_DEVICE;
+  // one warp's ring and staged rows must fit a block's shared memory
+  if (!fw2v::launch_fits(p)) return FW2V_ERR_ARGUMENT;
+  if (n_blocks == 0) return FW2V_OK;
   float* scratch = nullptr;
   fw2v_status s = scratch_address(dev, &scratch);
   if (s != FW2V_OK) return s;
@@ -66,14 +76,9 @@ extern "C" fw2v_status fw2v_kernel_batch_noalloc(float* syn0, float* syn1neg, co
   s = fw2v::seam_state(dev, &error_word, &table, &sms);
   if (s != FW2V_OK) return s;
 
-  fw2v::TrainParams p{};
   p.syn0 = syn0;
   p.syn1neg = syn1neg;
-  p.pitch = pitch;
   p.vocab = vocab_size;
-  p.d = layer_size;
-  p.window = window;
-  p.negative = negative;
   p.sigmoid = 0;
   p.ids = sen;
   p.negs = neg;

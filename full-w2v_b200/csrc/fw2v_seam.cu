@@ -15,6 +15,7 @@ extern "C" void fw2v_exp_table(float* t);
 
 namespace fw2v {
 cudaError_t launch_train(const TrainParams& p, int num_sms, cudaStream_t st);
+bool launch_fits(const TrainParams& p);
 size_t train_smem_bytes(int window, int64_t pitch, int warps, int r, bool prefetch, int elem);
 int64_t train_scratch_warps(int num_sms);
 }  // namespace fw2v
@@ -82,6 +83,7 @@ extern "C" fw2v_status fw2v_kernel_batch(float* syn0, float* syn1neg, const int3
   p.work_counter = nullptr;
   p.deterministic = 0;
   p.bf16 = 0;
+  if (!fw2v::launch_fits(p)) return FW2V_ERR_ARGUMENT;
   void* addr = nullptr;
   if (cudaGetSymbolAddress(&addr, g_seam_error) != cudaSuccess) return FW2V_ERR_CUDA;
   p.error_flag = (int*)addr;

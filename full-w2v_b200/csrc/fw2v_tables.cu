@@ -141,4 +141,24 @@ cudaError_t launch_validate_ids(const int32_t* ids, int64_t n, int64_t vocab, in
   return cudaGetLastError();
 }
 
+// A device-resident corpus: the stream ends with the 0 after its last word and
+// every chunk starts inside it (the checks fw2v_load_corpus makes on the host).
+__global__ void check_corpus_kernel(const int32_t* stream, int64_t len, const int64_t* chunk_off, int64_t n,
+                                    int* flag) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  bool bad = t == 0 && stream[len - 1] != 0;
+  for (int64_t i = t; i < n; i += stride) {
+    const int64_t o = chunk_off[i];
+    bad |= o < 0 || o >= len;
+  }
+  if (bad) atomicExch(flag, 1);
+}
+
+cudaError_t launch_check_corpus(const int32_t* stream, int64_t len, const int64_t* chunk_off, int64_t n, int* flag,
+                                cudaStream_t st) {
+  check_corpus_kernel<<<148 * 2, 256, 0, st>>>(stream, len, chunk_off, n, flag);
+  return cudaGetLastError();
+}
+
 }  // namespace fw2v

@@ -64,6 +64,7 @@ int64_t train_scratch_warps(int num_sms) { return (int64_t)num_sms * 64; }
 // 384 elements (three 4-float vectors per lane).
 template <int VEC, int NV>
 static cudaError_t launch_rt(const TrainParams& p, int r, int num_sms, size_t smem, cudaStream_t st) {
+  // smem: shared memory of one warp
   if (p.bf16) {
     if constexpr (NV <= 3) {
       return p.sigmoid == 0 ? launch_r<bf16_t, VEC, NV, 0>(p, r, num_sms, smem, st)
@@ -76,10 +77,21 @@ static cudaError_t launch_rt(const TrainParams& p, int r, int num_sms, size_t sm
                         : launch_r<float, VEC, NV, 1>(p, r, num_sms, smem, st);
 }
 
+// Shared memory of one warp of a launch of the training kernel.
+size_t launch_warp_smem(const TrainParams& p) {
+  const LaunchShape s = choose_shape(p.d, p.negative);
+  return train_smem_bytes(p.window, p.pitch, 1, s.r, p.prefetch != 0, p.bf16 ? 2 : 4);
+}
+
+// Whether one warp of a launch of p fits a block's shared memory (launch_t
+// takes 4, 2 or 1 warps per block, as many as fit).
+bool launch_fits(const TrainParams& p) {
+  return train_block_warps(launch_warp_smem(p), sizeof(TrainParams) + 64, 1) == 1;
+}
+
 cudaError_t launch_train(const TrainParams& p, int num_sms, cudaStream_t st) {
   const LaunchShape s = choose_shape(p.d, p.negative);
-  const size_t smem = train_smem_bytes(p.window, p.pitch, p.deterministic ? 1 : kWarpsPerBlock, s.r,
-                                       p.prefetch != 0, p.bf16 ? 2 : 4);
+  const size_t smem = launch_warp_smem(p);
   if (s.vec == 2) return launch_rt<2, 1>(p, s.r, num_sms, smem, st);
   switch (s.nv) {
     case 1: return launch_rt<4, 1>(p, s.r, num_sms, smem, st);

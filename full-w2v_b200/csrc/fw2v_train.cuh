@@ -477,15 +477,20 @@ __device__ __forceinline__ void row_add_delta(float* row, const Row<VEC, NV>& a,
   row_add_delta(row, a, b, lane, d);
 }
 
+// Lane partial of a dot product with the packed FP32x2 FMA of sm_100 (two
+// IEEE single-rounding FMAs per instruction): elements j and j+1 of every
+// vector (j even) go to two running sums, "even" and "odd", each a product
+// then FMAs in vector order; the lane's partial is even + odd.
 template <int VEC, int NV>
 __device__ __forceinline__ float row_dot(const Row<VEC, NV>& a, const Row<VEC, NV>& b) {
-  float p = __fmul_rn(a.x[0][0], b.x[0][0]);
+  float2 p = __fmul2_rn(make_float2(a.x[0][0], a.x[0][1]), make_float2(b.x[0][0], b.x[0][1]));
 #pragma unroll
   for (int i = 0; i < NV; i++)
 #pragma unroll
-    for (int j = 0; j < VEC; j++)
-      if (i != 0 || j != 0) p = __fmaf_rn(a.x[i][j], b.x[i][j], p);
-  return p;
+    for (int j = 0; j < VEC; j += 2)
+      if (i != 0 || j != 0)
+        p = __ffma2_rn(make_float2(a.x[i][j], a.x[i][j + 1]), make_float2(b.x[i][j], b.x[i][j + 1]), p);
+  return __fadd_rn(p.x, p.y);
 }
 
 __device__ __forceinline__ float warp_sum(float p) {
@@ -494,16 +499,23 @@ __device__ __forceinline__ float warp_sum(float p) {
   return p;
 }
 
-// v += g*o and o += g*v_old, elementwise with single-rounding FMAs.
+// v += g*o and o += g*v_old, elementwise with single-rounding FMAs, two
+// elements per packed FP32x2 FMA.
 template <int VEC, int NV>
 __device__ __forceinline__ void row_update(Row<VEC, NV>& v, Row<VEC, NV>& o, float g) {
+  const float2 g2 = make_float2(g, g);
 #pragma unroll
   for (int i = 0; i < NV; i++)
 #pragma unroll
-    for (int j = 0; j < VEC; j++) {
-      const float vo = v.x[i][j];
-      v.x[i][j] = __fmaf_rn(g, o.x[i][j], vo);
-      o.x[i][j] = __fmaf_rn(g, vo, o.x[i][j]);
+    for (int j = 0; j < VEC; j += 2) {
+      const float2 vo = make_float2(v.x[i][j], v.x[i][j + 1]);
+      const float2 oo = make_float2(o.x[i][j], o.x[i][j + 1]);
+      const float2 vn = __ffma2_rn(g2, oo, vo);
+      const float2 on = __ffma2_rn(g2, vo, oo);
+      v.x[i][j] = vn.x;
+      v.x[i][j + 1] = vn.y;
+      o.x[i][j] = on.x;
+      o.x[i][j + 1] = on.y;
     }
 }
 
@@ -1180,22 +1192,40 @@ __global__ void __launch_bounds__(128) heldout_loss_kernel(TrainParams p, double
 
 // Launch of one (VEC, NV) shape for any stage count R (instantiated per shape
 // in fw2v_train_<shape>.cu so the shapes compile in parallel).
+// Warps per block of a launch whose warps need warp_smem bytes of dynamic
+// shared memory each, beside `static_smem` bytes of the kernel's own: 4, or 2
+// or 1 where 4 do not fit a block (wide rows with long windows); 0 if not
+// even one does.  The kernel takes its warp count from blockDim.
+inline int train_block_warps(size_t warp_smem, size_t static_smem, int deterministic) {
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return 0;
+  int warps = deterministic ? 1 : kWarpsPerBlock;
+  while (warps > 1 && (size_t)warps * warp_smem + static_smem > (size_t)optin) warps /= 2;
+  return warp_smem + static_smem <= (size_t)optin ? warps : 0;
+}
+
 template <typename T, int VEC, int NV, int R, int SIG>
-cudaError_t launch_t(const TrainParams& p, int num_sms, size_t smem, cudaStream_t st) {
+cudaError_t launch_t(const TrainParams& p, int num_sms, size_t warp_smem, cudaStream_t st) {
   auto kern = sgns_train_kernel<T, VEC, NV, R, SIG>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, kern);
+  if (e != cudaSuccess) return e;
+  const int warps = train_block_warps(warp_smem, fa.sharedSizeBytes, p.deterministic);
+  if (warps < 1) return cudaErrorInvalidValue;
+  const size_t smem = (size_t)warps * warp_smem;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int blocks = 1;
-  int threads = kWarpsPerBlock * 32;
-  if (p.deterministic) {
-    threads = 32;
-  } else {
+  const int threads = warps * 32;
+  if (!p.deterministic) {
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     blocks = per_sm * num_sms;
-    const int64_t cap = p.scratch_warps / kWarpsPerBlock;
+    const int64_t cap = p.scratch_warps / warps;
     if (blocks > cap) blocks = (int)cap;
     if (blocks < 1) return cudaErrorInvalidConfiguration;
   }
@@ -1206,16 +1236,16 @@ cudaError_t launch_t(const TrainParams& p, int num_sms, size_t smem, cudaStream_
 // Stage counts compiled per shape: rows of up to 3 vectors per lane pipeline
 // up to 8 targets; wider rows (d > 384) sweep targets one at a time.
 template <typename T, int VEC, int NV, int SIG>
-cudaError_t launch_r(const TrainParams& p, int r, int num_sms, size_t smem, cudaStream_t st) {
+cudaError_t launch_r(const TrainParams& p, int r, int num_sms, size_t warp_smem, cudaStream_t st) {
   if constexpr (NV >= 4) {
-    return launch_t<T, VEC, NV, 1, SIG>(p, num_sms, smem, st);
+    return launch_t<T, VEC, NV, 1, SIG>(p, num_sms, warp_smem, st);
   } else {
     switch (r) {
-      case 1: return launch_t<T, VEC, NV, 1, SIG>(p, num_sms, smem, st);
-      case 2: return launch_t<T, VEC, NV, 2, SIG>(p, num_sms, smem, st);
-      case 4: return launch_t<T, VEC, NV, 4, SIG>(p, num_sms, smem, st);
-      case 6: return launch_t<T, VEC, NV, 6, SIG>(p, num_sms, smem, st);
-      default: return launch_t<T, VEC, NV, 8, SIG>(p, num_sms, smem, st);
+      case 1: return launch_t<T, VEC, NV, 1, SIG>(p, num_sms, warp_smem, st);
+      case 2: return launch_t<T, VEC, NV, 2, SIG>(p, num_sms, warp_smem, st);
+      case 4: return launch_t<T, VEC, NV, 4, SIG>(p, num_sms, warp_smem, st);
+      case 6: return launch_t<T, VEC, NV, 6, SIG>(p, num_sms, warp_smem, st);
+      default: return launch_t<T, VEC, NV, 8, SIG>(p, num_sms, warp_smem, st);
     }
   }
 }

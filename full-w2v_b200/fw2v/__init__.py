@@ -72,17 +72,18 @@ class TuneReport(C.Structure):
 # Every entry point declared in include/fw2v.h (tests check the library exports them all).
 EXPORTS = [
     "fw2v_config_default", "fw2v_create", "fw2v_destroy", "fw2v_set_vocab", "fw2v_load_corpus",
-    "fw2v_sample_epoch", "fw2v_epoch_sample_sizes", "fw2v_epoch_samples", "fw2v_train_sampled",
+    "fw2v_load_corpus_device", "fw2v_sample_epoch", "fw2v_epoch_sample_sizes", "fw2v_epoch_samples", "fw2v_train_sampled",
     "fw2v_train_epoch", "fw2v_train", "fw2v_words_trained", "fw2v_get_syn0", "fw2v_get_syn1neg",
     "fw2v_set_tables", "fw2v_train_sentences", "fw2v_heldout_loss", "fw2v_kernel_batch",
     "fw2v_kernel_batch_error", "fw2v_lane_layout", "fw2v_exp_table", "fw2v_unigram_firsts",
     "fw2v_get_unigram", "fw2v_status_string", "fw2v_last_error", "fw2v_version", "fw2v_stream",
     "fw2v_kernel_batch_noalloc", "fw2v_reorder_chunks",
     "fw2v_batch_config_default", "fw2v_batch_create", "fw2v_batch_destroy", "fw2v_batch_last_error",
-    "fw2v_batch_add_job", "fw2v_batch_set_shape", "fw2v_batch_get_shape", "fw2v_batch_set_launch",
+    "fw2v_batch_add_job", "fw2v_batch_add_job_device", "fw2v_batch_set_shape", "fw2v_batch_get_shape", "fw2v_batch_set_launch",
     "fw2v_batch_get_launch", "fw2v_batch_tune", "fw2v_batch_train", "fw2v_batch_train_epochs",
     "fw2v_batch_job_words",
-    "fw2v_batch_get_syn0", "fw2v_batch_get_syn1neg",
+    "fw2v_batch_get_syn0", "fw2v_batch_get_syn1neg", "fw2v_neighbours", "fw2v_random_walks",
+    "fw2v_relabel_stream",
 ]
 
 _lib = None
@@ -103,6 +104,7 @@ def lib() -> C.CDLL:
             "fw2v_destroy": (None, [H]),
             "fw2v_set_vocab": (C.c_int, [H, P, I64, U64]),
             "fw2v_load_corpus": (C.c_int, [H, P, I64, P, I64]),
+            "fw2v_load_corpus_device": (C.c_int, [H, P, I64, P, I64]),
             "fw2v_reorder_chunks": (C.c_int, [H, P, I64]),
             "fw2v_sample_epoch": (C.c_int, [H]),
             "fw2v_epoch_sample_sizes": (C.c_int, [H, C.POINTER(I64), C.POINTER(I64)]),
@@ -137,6 +139,8 @@ def lib() -> C.CDLL:
             "fw2v_batch_last_error": (C.c_char_p, [H]),
             "fw2v_batch_add_job": (C.c_int, [H, C.POINTER(Config), P, I64, U64, P, I64, P, I64,
                                              C.POINTER(I32)]),
+            "fw2v_batch_add_job_device": (C.c_int, [H, C.POINTER(Config), P, I64, U64, P, I64, P, I64,
+                                                    C.POINTER(I32)]),
             "fw2v_batch_set_shape": (C.c_int, [H, I32, I32, I32, I32, I32]),
             "fw2v_batch_get_shape": (C.c_int, [H, I32, C.POINTER(I32), C.POINTER(I32), C.POINTER(I32),
                                                C.POINTER(I32)]),
@@ -148,6 +152,9 @@ def lib() -> C.CDLL:
             "fw2v_batch_job_words": (C.c_int, [H, I32, C.POINTER(U64), C.POINTER(U64)]),
             "fw2v_batch_get_syn0": (C.c_int, [H, I32, P, I64]),
             "fw2v_batch_get_syn1neg": (C.c_int, [H, I32, P, I64]),
+            "fw2v_neighbours": (C.c_int, [P, I32, I64, I32, P, I64, P, I64, I32, P, P, P]),
+            "fw2v_random_walks": (C.c_int, [P, P, I64, P, I64, I32, U64, P, P]),
+            "fw2v_relabel_stream": (C.c_int, [P, I64, P, I64, P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -159,6 +166,21 @@ def lib() -> C.CDLL:
 
 def _p(a: np.ndarray | None):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _on_device(a) -> bool:
+    return type(a).__module__.startswith("torch") and a.is_cuda
+
+
+def _device_pair(stream, chunk_off):
+    """A device stream (int32) and its chunk offsets (int64) as contiguous CUDA
+    tensors on the stream's device (offsets given on the host are copied)."""
+    import torch
+    st = stream.to(torch.int32).contiguous()
+    co = chunk_off if _on_device(chunk_off) else torch.from_numpy(np.ascontiguousarray(chunk_off, np.int64))
+    co = co.to(device=st.device, dtype=torch.int64).contiguous()
+    torch.cuda.current_stream(st.device).synchronize()  # the tensors are written before the library reads them
+    return st, co
 
 
 def default_config(**overrides) -> Config:
@@ -232,7 +254,15 @@ class Trainer:
                     "set_vocab")
         self.vocab_size = len(counts)
 
-    def load_corpus(self, stream: np.ndarray, chunk_off: np.ndarray):
+    def load_corpus(self, stream, chunk_off):
+        """Token stream and chunk offsets: numpy arrays (host memory), or CUDA
+        tensors (int32 / int64), which are loaded on the device without a host
+        round trip (fw2v_load_corpus_device)."""
+        if _on_device(stream):
+            st, co = _device_pair(stream, chunk_off)
+            self._check(lib().fw2v_load_corpus_device(self._h, st.data_ptr(), st.numel(), co.data_ptr(),
+                                                      co.numel()), "load_corpus_device")
+            return
         stream = np.ascontiguousarray(stream, np.int32)
         chunk_off = np.ascontiguousarray(chunk_off, np.int64)
         self._check(lib().fw2v_load_corpus(self._h, _p(stream), len(stream), _p(chunk_off),
@@ -384,15 +414,22 @@ class Batch:
             msg = lib().fw2v_batch_last_error(self._h)
             raise Fw2vError(st, f"{what}: {msg.decode() if msg else ''}")
 
-    def add_job(self, config: Config, counts: np.ndarray, train_words: int, stream: np.ndarray,
-                chunk_off: np.ndarray) -> int:
+    def add_job(self, config: Config, counts: np.ndarray, train_words: int, stream, chunk_off) -> int:
+        """A job; its stream and chunk offsets as numpy arrays or as CUDA
+        tensors (loaded on the device, fw2v_batch_add_job_device)."""
         counts = np.ascontiguousarray(counts, np.uint32)
-        stream = np.ascontiguousarray(stream, np.int32)
-        chunk_off = np.ascontiguousarray(chunk_off, np.int64)
         j = C.c_int32()
-        self._check(lib().fw2v_batch_add_job(self._h, C.byref(config), _p(counts), len(counts), int(train_words),
-                                             _p(stream), len(stream), _p(chunk_off), len(chunk_off),
-                                             C.byref(j)), "batch_add_job")
+        if _on_device(stream):
+            st, co = _device_pair(stream, chunk_off)
+            self._check(lib().fw2v_batch_add_job_device(self._h, C.byref(config), _p(counts), len(counts),
+                                                        int(train_words), st.data_ptr(), st.numel(), co.data_ptr(),
+                                                        co.numel(), C.byref(j)), "batch_add_job_device")
+        else:
+            stream = np.ascontiguousarray(stream, np.int32)
+            chunk_off = np.ascontiguousarray(chunk_off, np.int64)
+            self._check(lib().fw2v_batch_add_job(self._h, C.byref(config), _p(counts), len(counts),
+                                                 int(train_words), _p(stream), len(stream), _p(chunk_off),
+                                                 len(chunk_off), C.byref(j)), "batch_add_job")
         self.jobs.append((config, len(counts)))
         return j.value
 

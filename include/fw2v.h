@@ -115,6 +115,13 @@ fw2v_status fw2v_set_vocab(fw2v_handle* h, const uint32_t* counts, int64_t vocab
  * streams' LCG and learning-rate state and the epoch count. */
 fw2v_status fw2v_load_corpus(fw2v_handle* h, const int32_t* stream, int64_t stream_len,
                              const int64_t* chunk_off, int64_t n_chunks);
+/* The same from device memory (both arrays device pointers, e.g. a corpus
+ * generated on the GPU): checked by a kernel (trailing 0, chunk offsets inside
+ * the stream, ids in [0, V)) and copied on the device; no host round trip.
+ * The replacement of createGlobalStream's host array for corpora that already
+ * live on the GPU (improved_driver_functions.cpp:244-281). */
+fw2v_status fw2v_load_corpus_device(fw2v_handle* h, const int32_t* stream, int64_t stream_len,
+                                    const int64_t* chunk_off, int64_t n_chunks);
 
 /* Replace the order of the stored chunks without touching the streams' LCG and
  * learning-rate state: the reference's -epoch-shuffle, which permutes its
@@ -178,18 +185,22 @@ fw2v_status fw2v_kernel_batch(float* syn0, float* syn1neg, const int32_t* sen, c
 /* fw2v_kernel_batch without any device allocation.  No counterpart in the
  * reference: FULL-W2V allocates all of its buffers up front in its driver.
  *
- * For callers that must not allocate device memory: code that runs while a
- * stream is being captured into a CUDA graph (cudaMalloc/cudaFree cannot be
- * captured and cudaFree synchronises the device), programs whose device memory
- * is owned entirely by a framework's pooling allocator, and latency-bound loops
- * that cannot absorb an allocator call.  Arguments and results are those of
+ * For callers that cannot allocate device memory: a host program whose device
+ * memory is owned entirely by a framework's pooling allocator (a direct
+ * cudaMalloc would bypass the pool's accounting and can fail once the pool
+ * holds the device), a plugin host that hands the library its buffers under a
+ * fixed memory budget, and latency-bound loops in which cudaMalloc/cudaFree
+ * would stall or synchronise the device.  Arguments and results are those of
  * fw2v_kernel_batch.  The per-warp scratch the kernel needs (each context row's
  * value when it entered the window) lives in a fixed array of
  * FW2V_NOALLOC_SCRATCH_BYTES inside the library, which every GPU that loads the
  * library keeps until the process exits; (2*window+1) * pitch * 4 bytes per warp
  * of up to FW2V_NOALLOC_SCRATCH_BYTES in total cap the number of warps working
  * concurrently.  A request needing more than that for one block of 4 warps is
- * rejected with FW2V_ERR_TOO_LARGE before anything runs.
+ * rejected with FW2V_ERR_TOO_LARGE, and one whose per-warp shared memory (the
+ * ring of 2*window+1 rows and the staged target rows, about
+ * (2*window + 12) * pitch * 4 bytes) does not fit a block with
+ * FW2V_ERR_ARGUMENT, both before anything runs.
  *
  * The first call on a device looks up the array's device address and loads the
  * sigmoid table; make that first call before any stream capture.  All calls
@@ -224,6 +235,38 @@ int fw2v_unigram_firsts(const uint32_t* counts, int64_t vocab_size, int64_t tabl
                         int64_t* firsts);
 /* Copy n entries of the device unigram table starting at index `first`. */
 fw2v_status fw2v_get_unigram(fw2v_handle* h, int64_t first, int64_t n, int32_t* out);
+
+/* Nearest neighbours by cosine similarity, the evaluator behind same-label
+ * precision@10 (the reference scores its vectors offline with public
+ * word-similarity sets, analysis/hyperwords; the synthetic corpora carry a
+ * planted label per word instead).  `table` holds rows of `pitch` elements
+ * (FP32, or bfloat16 bits with FW2V_BF16), the first layer_size (<= 512) used;
+ * cand[0..n_cand) are the rows searched; query q is candidate queries[q].  For
+ * each query: the k (<= 32, < n_cand) most similar other candidates, most
+ * similar first, as candidate indices in out_idx[q*k..] and cosines in
+ * out_sim[q*k..]; ties go to the lower candidate index.  Device pointers;
+ * asynchronous on `stream` (a cudaStream_t); takes its scratch from the
+ * stream-ordered allocator. */
+fw2v_status fw2v_neighbours(const void* table, int32_t precision, int64_t pitch, int32_t layer_size,
+                            const int32_t* cand, int64_t n_cand, const int32_t* queries,
+                            int64_t n_queries, int32_t k, int32_t* out_idx, float* out_sim,
+                            void* stream);
+
+/* Graph-walk corpora generated on the device (the reference reads walk
+ * corpora as text, one walk per line with -cache-eos, through
+ * createGlobalStream, improved_driver_functions.cpp:244-281; these write the
+ * same token stream in device memory).
+ * fw2v_random_walks: n_walks uniform random walks of walk_len nodes on a graph
+ * in CSR form (offs[0..nodes], dst[offs[0]..offs[nodes]), device pointers),
+ * walk w starting at starts[w]; each step takes a uniform neighbour chosen by
+ * a counter-based hash of (seed, w, step), a node without neighbours stays.
+ * Writes node ids, walk w at out[w*(walk_len+1) ..], then -1 after each walk.
+ * fw2v_relabel_stream: such a stream in place: node x -> vocab_of[x], every
+ * negative entry -> 0 (</s>). */
+fw2v_status fw2v_random_walks(const int64_t* offs, const int32_t* dst, int64_t nodes, const int32_t* starts,
+                              int64_t n_walks, int32_t walk_len, uint64_t seed, int32_t* out, void* stream);
+fw2v_status fw2v_relabel_stream(int32_t* stream, int64_t n, const int32_t* vocab_of, int64_t nodes,
+                                void* cuda_stream);
 
 /* The handle's CUDA stream (a cudaStream_t), on which every kernel of the
  * handle runs; lets a caller time or order its own work against the epochs. */
@@ -285,6 +328,12 @@ const char* fw2v_batch_last_error(fw2v_batch* b);
 fw2v_status fw2v_batch_add_job(fw2v_batch* b, const fw2v_config* cfg, const uint32_t* counts, int64_t vocab_size,
                                uint64_t train_words, const int32_t* stream, int64_t stream_len,
                                const int64_t* chunk_off, int64_t n_chunks, int32_t* job);
+/* fw2v_batch_add_job with the corpus in device memory (stream and chunk_off
+ * device pointers, checked on the device as fw2v_load_corpus_device does);
+ * counts stay in host memory. */
+fw2v_status fw2v_batch_add_job_device(fw2v_batch* b, const fw2v_config* cfg, const uint32_t* counts,
+                                      int64_t vocab_size, uint64_t train_words, const int32_t* stream,
+                                      int64_t stream_len, const int64_t* chunk_off, int64_t n_chunks, int32_t* job);
 
 /* A job's kernel shape: the lane vector width and vectors per lane (2 x 1:
  * 32 lanes of 2 floats cover d <= 64; 4 x 1: d <= 128, 16 lanes suffice for

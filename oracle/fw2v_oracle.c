@@ -227,34 +227,38 @@ static double grad_f64(const orc_train_cfg* cfg, double x, int label, float alph
   return label ? (double)alpha / (1.0 + exp(x)) : -(double)alpha / (1.0 + exp(-x));
 }
 
-/* Dot product with the CUDA kernel's order: lane l of 32 accumulates elements
- * ((i*32+l)*vec + j), i < nv, j < vec, first a product then FMAs; lanes are
- * combined by the xor tree with masks 16, 8, 4, 2, 1 (zero beyond d). */
+/* Dot product with the CUDA kernel's order: lane l of 32 holds elements
+ * ((i*32+l)*vec + j), i < nv, j < vec, and keeps two running sums, "even"
+ * (j = 0, 2) and "odd" (j = 1, 3), each first a product then FMAs in (i, j)
+ * order (the kernel's packed FP32x2 FMAs); the lane's partial is even + odd,
+ * and lanes are combined by the xor tree with masks 16, 8, 4, 2, 1 (zero
+ * beyond d). */
 static float dot_f32(const orc_train_cfg* cfg, const float* a, const float* b) {
   float part[32];
   for (int l = 0; l < 32; l++) {
-    float p = 0.0f;
+    float pe = 0.0f, po = 0.0f;
     int first = 1;
     for (int i = 0; i < cfg->nv; i++) {
-      for (int j = 0; j < cfg->vec; j++) {
+      for (int j = 0; j < cfg->vec; j += 2) {
         int e = (i * 32 + l) * cfg->vec + j;
-        float x = e < cfg->d ? a[e] : 0.0f;
-        float y = e < cfg->d ? b[e] : 0.0f;
+        float x0 = e < cfg->d ? a[e] : 0.0f, y0 = e < cfg->d ? b[e] : 0.0f;
+        float x1 = e + 1 < cfg->d ? a[e + 1] : 0.0f, y1 = e + 1 < cfg->d ? b[e + 1] : 0.0f;
         if (first) {
-          p = x * y;
+          pe = x0 * y0;
+          po = x1 * y1;
           first = 0;
         } else {
-          p = fmaf(x, y, p);
+          pe = fmaf(x0, y0, pe);
+          po = fmaf(x1, y1, po);
         }
       }
     }
-    part[l] = p;
+    part[l] = pe + po;
   }
-  for (int m = 16; m >= 1; m >>= 1) {
-    float nxt[32];
-    for (int l = 0; l < 32; l++) nxt[l] = part[l] + part[l ^ m];
-    memcpy(part, nxt, sizeof(part));
-  }
+  /* Lanes l and l^m add the same two values, so after each level the lanes of
+   * a group agree and lane 0's sums are the tree: part[l] + part[l + m]. */
+  for (int m = 16; m >= 1; m >>= 1)
+    for (int l = 0; l < m; l++) part[l] = part[l] + part[l + m];
   return part[0];
 }
 

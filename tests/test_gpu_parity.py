@@ -412,3 +412,34 @@ def test_bf16_learns_like_fp32():
                 if det:
                     losses[prec] = after
     assert abs(losses[fw2v.BF16] - losses[fw2v.FP32]) <= 0.005 * losses[fw2v.FP32]
+
+
+@pytest.mark.parametrize("d,W", [(1024, 5), (384, 15), (600, 8)])
+def test_wide_rows_long_windows_hogwild_bit_exact(d, W):
+    """Layer sizes and windows where four warps' shared memory does not fit a
+    block (d=1024 with W=5 needs 4 x 61 KB): the launch takes two warps per
+    block, or one.  Hogwild (deterministic=0) on sentences that each draw ids
+    and negatives from their own rows, so any warp order gives the oracle's
+    result bit for bit."""
+    K, n, rows, msl = 5, 64, 30, 40
+    V = 1 + n * rows
+    rng = np.random.default_rng(d + W)
+    lens = rng.integers(1, msl + 1, n).astype(np.int32)
+    base = 1 + np.arange(n) * rows
+    ids = np.concatenate([base[s] + rng.integers(0, rows, lens[s]) for s in range(n)]).astype(np.int32)
+    owner = np.repeat(base, lens)
+    negs = (owner[:, None] + rng.integers(0, rows, (len(ids), K))).astype(np.int32).ravel()
+    alphas = np.full(n, 0.025, np.float32)
+    counts = np.arange(V, 0, -1).astype(np.uint32)
+    vec, nv, _ = fw2v.lane_layout(d)
+    with fw2v.Trainer(fw2v.default_config(layer_size=d, window=W, negative=K, threads=1, deterministic=0)) as t:
+        t.set_vocab(counts, int(counts.sum()))
+        syn1 = (rng.standard_normal((V, d)) * 0.05).astype(np.float32)
+        t.set_tables(None, syn1)
+        syn0 = t.syn0()
+        t.train_sentences(lens, alphas, ids, negs)
+        got0, got1 = t.syn0(), t.syn1neg()
+    O.train(syn0, syn1, lens, alphas, ids, negs, d=d, window=W, negative=K, sigmoid="table",
+            precision=32, vec=vec, nv=nv)
+    np.testing.assert_array_equal(got0, syn0)
+    np.testing.assert_array_equal(got1, syn1)
