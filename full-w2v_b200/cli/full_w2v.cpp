@@ -26,6 +26,7 @@
 #include <cstring>
 #include <ctime>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -42,6 +43,7 @@ struct Options {
   int binary = 0, debug = 2, min_count = 5, layer_size = 100, epochs = 5, window = 5, negative = 5;
   int threads = -1, msl = 1000, sigmoid = FW2V_SIGMOID_TABLE, deterministic = 0, device = 0;
   int precision = FW2V_FP32, tune = 1;
+  int read_threads = 0;  // text reader threads (0: one per core, segments of >= 4 MB)
   unsigned long long seed = 0;
   float alpha = 0.025f, sample = 1e-3f;
   std::string jobs;  // manifest: one job's arguments per line, trained together
@@ -265,6 +267,137 @@ void create_stream(Corpus& c, const Vocab& v, const Mapped& f, int msl, bool cac
   c.stream.push_back(0);
 }
 
+// ---------------------------------------------------------------------------
+// Parallel text reader: the same vocabulary and token stream as learn_vocab /
+// create_stream, with the file cut into segments at line starts and each
+// segment read by its own thread.  The word reader keeps no state across a
+// line start, so every segment reads the words the serial pass reads there.
+// Each thread counts its words with the position of their first occurrence;
+// merged, the insertion order of the serial pass is the order of first
+// occurrence, which the stable sort by count keeps for ties.  A vocabulary
+// that would reach the serial pass's ReduceVocab threshold is read serially.
+// ---------------------------------------------------------------------------
+struct Segments {
+  std::vector<uint64_t> begin, end;
+};
+
+// n segments of f starting at line starts (fewer if lines are long).
+Segments cut_segments(const Mapped& f, int n) {
+  Segments s;
+  uint64_t pos = 0;
+  for (int k = 0; k < n && pos < f.size; k++) {
+    uint64_t e = k + 1 == n ? f.size : std::max(pos, f.size / n * (k + 1));
+    while (e < f.size && f.data[e - 1] != '\n') e++;
+    if (e <= pos) continue;
+    s.begin.push_back(pos);
+    s.end.push_back(e);
+    pos = e;
+  }
+  return s;
+}
+
+int reader_threads(const Options& o, const Mapped& f) {
+  if (o.read_threads > 0) return o.read_threads;
+  const int cores = (int)std::max(1u, std::thread::hardware_concurrency());
+  return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)cores, f.size / (4u << 20)));
+}
+
+struct SegmentCounts {
+  std::unordered_map<std::string, std::pair<uint64_t, uint64_t>> words;  // count, first token index
+  uint64_t tokens = 0;
+};
+
+// Returns false (and leaves v untouched) when the vocabulary is too large for
+// the parallel pass.
+bool learn_vocab_parallel(Vocab& v, const Mapped& f, int min_count, int n, uint64_t* train_words) {
+  const Segments seg = cut_segments(f, n);
+  const size_t ns = seg.begin.size();
+  std::vector<SegmentCounts> part(ns);
+  std::vector<std::thread> pool;
+  for (size_t k = 0; k < ns; k++)
+    pool.emplace_back([&, k] {
+      std::string w;
+      SegmentCounts& c = part[k];
+      const uint64_t end = seg.end[k];
+      for (uint64_t pos = seg.begin[k]; pos < end;) {
+        read_word(w, f.data, end, &pos);
+        // the word that ends exactly at the end of the file is not counted
+        if (pos == end && end == f.size) break;
+        auto it = c.words.find(w);
+        if (it == c.words.end()) c.words.emplace(w, std::make_pair(1ull, c.tokens));
+        else it->second.first++;
+        c.tokens++;
+      }
+    });
+  for (auto& t : pool) t.join();
+  std::unordered_map<std::string, std::pair<uint64_t, uint64_t>> all;
+  uint64_t base = 0;
+  for (size_t k = 0; k < ns; k++) {
+    for (auto& kv : part[k].words) {
+      auto it = all.find(kv.first);
+      const uint64_t first = base + kv.second.second;
+      if (it == all.end()) all.emplace(kv.first, std::make_pair(kv.second.first, first));
+      else {
+        it->second.first += kv.second.first;
+        it->second.second = std::min(it->second.second, first);
+      }
+    }
+    base += part[k].tokens;
+    part[k].words.clear();
+  }
+  if ((int64_t)all.size() + 1 > (int64_t)(kVocabHashSize * 0.7)) return false;
+  std::vector<std::pair<uint64_t, const std::string*>> order;  // first occurrence, word
+  order.reserve(all.size());
+  for (auto& kv : all)
+    if (kv.first != "</s>") order.emplace_back(kv.second.second, &kv.first);
+  std::sort(order.begin(), order.end());
+  v.add("</s>");
+  auto eos = all.find("</s>");
+  v.counts[0] = eos == all.end() ? 0 : eos->second.first;
+  for (auto& o : order) {
+    const int i = v.add(*o.second);
+    v.counts[i] = all[*o.second].first;
+  }
+  *train_words = v.sort_and_cut(min_count) + 1;
+  return true;
+}
+
+// create_stream over segments read in parallel: each thread maps its words to
+// ids (in-vocabulary words only, "</s>" kept with -cache-eos); the chunk cuts,
+// which carry across segments, are made in one pass over the joined stream.
+void create_stream_parallel(Corpus& c, const Vocab& v, const Mapped& f, int msl, bool cache_eos, int n) {
+  const Segments seg = cut_segments(f, n);
+  const size_t ns = seg.begin.size();
+  std::vector<std::vector<int32_t>> part(ns);
+  std::vector<std::thread> pool;
+  for (size_t k = 0; k < ns; k++)
+    pool.emplace_back([&, k] {
+      std::string w;
+      const uint64_t end = seg.end[k];
+      for (uint64_t pos = seg.begin[k]; pos < end;) {
+        read_word(w, f.data, end, &pos);
+        const int id = v.find(w);
+        if (id < 0 || (!cache_eos && id == 0)) continue;
+        part[k].push_back(id);
+      }
+    });
+  for (auto& t : pool) t.join();
+  size_t total = 1;
+  for (auto& p : part) total += p.size();
+  c.stream.reserve(total);
+  for (auto& p : part) {
+    c.stream.insert(c.stream.end(), p.begin(), p.end());
+    std::vector<int32_t>().swap(p);
+  }
+  int64_t sent_length = 0;
+  for (size_t i = 0; i < c.stream.size(); i++) {
+    if (sent_length == 0) c.chunk_off.push_back((int64_t)i);
+    sent_length++;
+    if (c.stream[i] == 0 || sent_length >= msl) sent_length = 0;
+  }
+  c.stream.push_back(0);
+}
+
 // saveCorpusCache / saveCorpus (improved_driver_functions.cpp:293-318).
 bool save_corpus(const Corpus& c, const Vocab& v, uint64_t train_words, int msl, const std::string& path,
                  bool as_words) {
@@ -387,7 +520,8 @@ void usage(const char* prog) {
   printf("\t-sigmoid table|exact\tSigmoid: the reference's 1000-entry table (default) or exact\n");
   printf("\t-deterministic 0|1\tTrain sentences one at a time in stream order\n");
   printf("\t-precision fp32|bf16\tEmbedding tables in FP32 (default) or bfloat16 with stochastic rounding\n");
-  printf("\t-seed <int>\t\t0 (default): the reference's seeds; otherwise offsets every LCG start\n");
+  printf("\t-seed <int>\t\t0 (default): the reference's seeds; otherwise offsets every LCG start, and\n"
+         "\t\t\t\t-pre-shuffle / -epoch-shuffle use the library's seeded shuffle on the GPU\n");
   printf("** MANY JOBS **\n");
   printf("\t-jobs <file>\t\tTrain the jobs listed in <file> (one job's options per line, '#' comments)\n");
   printf("\t\t\t\ttogether on one GPU; -precision, -device, -deterministic apply to all\n");
@@ -395,6 +529,7 @@ void usage(const char* prog) {
   printf("** PARALLEL UTILIZATION **\n");
   printf("\t-thread(s) <int>\tSampling streams (the reference's CPU threads); default: one per 256 sentences\n");
   printf("\t-max-sentence-length, -msl <int>\tMaximum sentence length; default 1000\n");
+  printf("\t-read-threads <int>\tThreads reading the text file; default one per core (segments of >= 4 MB)\n");
   printf("\t-device <int>\t\tCUDA device; default 0\n");
   printf("\t-streams, -kernel-batch-size <int>\tAccepted for compatibility, unused\n");
   printf("\nExamples:\n%s -train data.txt -output vec.txt -size 128 -window 5 -sample 1e-4 -negative 5 -epoch 3\n\n",
@@ -443,6 +578,7 @@ bool parse(int argc, char** argv, Options& o) {
   if (const char* v = val("-device")) o.device = atoi(v);
   if (const char* v = val("-precision")) o.precision = !strcmp(v, "bf16") ? FW2V_BF16 : FW2V_FP32;
   if (const char* v = val("-seed")) o.seed = strtoull(v, nullptr, 10);
+  if (const char* v = val("-read-threads")) o.read_threads = atoi(v);
   if (const char* v = val("-jobs")) o.jobs = v;
   if (const char* v = val("-tune")) o.tune = atoi(v);
   return true;
@@ -489,7 +625,9 @@ int prepare(Options& o, Vocab& vocab, Corpus& corpus, uint64_t& train_words) {
         return 1;
       }
     } else {
-      train_words = learn_vocab(vocab, f, o.min_count);
+      const int n = reader_threads(o, f);
+      if (n <= 1 || !learn_vocab_parallel(vocab, f, o.min_count, n, &train_words))
+        train_words = learn_vocab(vocab, f, o.min_count);
     }
     if (o.recount) train_words = recount_vocab(vocab, f, o.min_count);
     if (!o.save_vocab.empty()) save_vocab(vocab, o.save_vocab);
@@ -499,7 +637,9 @@ int prepare(Options& o, Vocab& vocab, Corpus& corpus, uint64_t& train_words) {
         return 1;
       }
     } else {
-      create_stream(corpus, vocab, f, o.msl, o.cache_eos);
+      const int n = reader_threads(o, f);
+      if (n > 1) create_stream_parallel(corpus, vocab, f, o.msl, o.cache_eos, n);
+      else create_stream(corpus, vocab, f, o.msl, o.cache_eos);
     }
   } else {
     if (o.read_vocab.empty()) {
@@ -660,7 +800,12 @@ int main(int argc, char** argv) {
   if (!o.jobs.empty()) return run_jobs(o);
   if (const int r = prepare(o, vocab, corpus, train_words)) return r < 0 ? 0 : r;
   const int64_t n_chunks = (int64_t)corpus.chunk_off.size();
-  if (o.pre_shuffle) shuffle_chunks(corpus.chunk_off);
+  // -seed 0: the reference's libc rand() shuffles on the host; another seed:
+  // the library's seeded Fisher-Yates on the device, shuffle n keyed by
+  // (seed, n)
+  const bool device_shuffle = o.seed != 0;
+  auto shuffle_key = [&](uint64_t n) { return (uint64_t)o.seed + 0x9E3779B97F4A7C15ULL * (n + 1); };
+  if (o.pre_shuffle && !device_shuffle) shuffle_chunks(corpus.chunk_off);
 
   // InitNet + Train_SGNS through libfw2v
   const fw2v_config cfg = job_config(o);
@@ -674,6 +819,9 @@ int main(int argc, char** argv) {
   if ((st = fw2v_load_corpus(h, corpus.stream.data(), (int64_t)corpus.stream.size(), corpus.chunk_off.data(),
                              n_chunks)) != FW2V_OK)
     return fail_status("load_corpus", st, h);
+  uint64_t shuffles = 0;
+  if (o.pre_shuffle && device_shuffle && (st = fw2v_shuffle_chunks(h, shuffle_key(shuffles++))) != FW2V_OK)
+    return fail_status("shuffle_chunks", st, h);
 
   const double t0 = now_s();
   uint64_t words = 0;
@@ -682,7 +830,10 @@ int main(int argc, char** argv) {
     if (o.epoch_shuffle) {
       if ((st = fw2v_sample_epoch(h)) != FW2V_OK || (st = fw2v_train_sampled(h, &es)) != FW2V_OK)
         return fail_status("train", st, h);
-      if (e + 1 < o.epochs) {
+      if (e + 1 < o.epochs && device_shuffle) {
+        if ((st = fw2v_shuffle_chunks(h, shuffle_key(shuffles++))) != FW2V_OK)
+          return fail_status("shuffle_chunks", st, h);
+      } else if (e + 1 < o.epochs) {
         shuffle_chunks(corpus.chunk_off);
         if ((st = fw2v_reorder_chunks(h, corpus.chunk_off.data(), n_chunks)) != FW2V_OK)
           return fail_status("reorder_chunks", st, h);

@@ -28,6 +28,7 @@ int64_t train_scratch_warps(int num_sms);
 cudaError_t launch_validate_ids(const int32_t* ids, int64_t n, int64_t vocab, int* flag, cudaStream_t st);
 cudaError_t launch_check_corpus(const int32_t* stream, int64_t len, const int64_t* chunk_off, int64_t n, int* flag,
                                 cudaStream_t st);
+cudaError_t launch_fisher_yates(int64_t* a, int64_t n, uint64_t key, cudaStream_t st);
 cudaError_t launch_corpus_layout(const int32_t* stream, int64_t stream_len, const int64_t* chunk_off,
                                  int64_t n_chunks, int msl, int threads, int64_t* chunk_base,
                                  int64_t* stream_base, cudaStream_t st);
@@ -480,6 +481,26 @@ fw2v_status fw2v_reorder_chunks(fw2v_handle* h, const int64_t* chunk_off, int64_
   CK(h, cudaStreamSynchronize(h->stream));
   CK(h, cudaMemcpyAsync(h->chunk_off, chunk_off, n_chunks * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
   return layout_streams(h);
+}
+
+fw2v_status fw2v_shuffle_chunks(fw2v_handle* h, uint64_t key) {
+  if (!h) return FW2V_ERR_ARGUMENT;
+  if (!h->stream_ids) return fail(h, FW2V_ERR_STATE, "shuffle_chunks before load_corpus");
+  if (h->n_sampled != h->n_trained)
+    return fail(h, FW2V_ERR_STATE, "shuffle_chunks with a sampled epoch not yet trained");
+  CK(h, cudaSetDevice(h->cfg.device));
+  CK(h, cudaStreamSynchronize(h->sstream));
+  CK(h, launch_fisher_yates(h->chunk_off, h->n_chunks, key, h->stream));
+  return layout_streams(h);
+}
+
+fw2v_status fw2v_get_chunks(fw2v_handle* h, int64_t* chunk_off) {
+  if (!h || !chunk_off) return FW2V_ERR_ARGUMENT;
+  if (!h->stream_ids) return fail(h, FW2V_ERR_STATE, "get_chunks before load_corpus");
+  CK(h, cudaSetDevice(h->cfg.device));
+  CK(h, cudaMemcpyAsync(chunk_off, h->chunk_off, h->n_chunks * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  return FW2V_OK;
 }
 
 fw2v_status fw2v_sample_epoch(fw2v_handle* h) {

@@ -155,6 +155,48 @@ __global__ void check_corpus_kernel(const int32_t* stream, int64_t len, const in
   if (bad) atomicExch(flag, 1);
 }
 
+// Seeded Fisher-Yates over n chunk offsets, on the device: for i = n-1 down
+// to 1, j = the high 64 bits of mix64(key ^ mix64(i)) * (i + 1), swap a[i]
+// and a[j].  The draws do not depend on the array, and the swaps are applied
+// in order by one thread, on a copy in shared memory when the array fits
+// there (use_smem), in place otherwise.
+__global__ void fisher_yates_kernel(int64_t* a, int64_t n, uint64_t key, int use_smem) {
+  extern __shared__ int64_t sa[];
+  if (use_smem) {
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) sa[i] = a[i];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    int64_t* x = use_smem ? sa : a;
+    for (int64_t i = n - 1; i > 0; i--) {
+      const int64_t j = (int64_t)__umul64hi(mix64(key ^ mix64((uint64_t)i)), (uint64_t)(i + 1));
+      const int64_t t = x[i];
+      x[i] = x[j];
+      x[j] = t;
+    }
+  }
+  if (use_smem) {
+    __syncthreads();
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) a[i] = sa[i];
+  }
+}
+
+cudaError_t launch_fisher_yates(int64_t* a, int64_t n, uint64_t key, cudaStream_t st) {
+  if (n < 2) return cudaSuccess;
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  const size_t bytes = (size_t)n * sizeof(int64_t);
+  const int use_smem = bytes <= (size_t)optin;
+  if (use_smem) {
+    e = cudaFuncSetAttribute(fisher_yates_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+  }
+  fisher_yates_kernel<<<1, 1024, use_smem ? bytes : 0, st>>>(a, n, key, use_smem);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_check_corpus(const int32_t* stream, int64_t len, const int64_t* chunk_off, int64_t n, int* flag,
                                 cudaStream_t st) {
   check_corpus_kernel<<<148 * 2, 256, 0, st>>>(stream, len, chunk_off, n, flag);

@@ -77,7 +77,7 @@ EXPORTS = [
     "fw2v_set_tables", "fw2v_train_sentences", "fw2v_heldout_loss", "fw2v_kernel_batch",
     "fw2v_kernel_batch_error", "fw2v_lane_layout", "fw2v_exp_table", "fw2v_unigram_firsts",
     "fw2v_get_unigram", "fw2v_status_string", "fw2v_last_error", "fw2v_version", "fw2v_stream",
-    "fw2v_kernel_batch_noalloc", "fw2v_reorder_chunks",
+    "fw2v_kernel_batch_noalloc", "fw2v_reorder_chunks", "fw2v_shuffle_chunks", "fw2v_get_chunks",
     "fw2v_batch_config_default", "fw2v_batch_create", "fw2v_batch_destroy", "fw2v_batch_last_error",
     "fw2v_batch_add_job", "fw2v_batch_add_job_device", "fw2v_batch_set_shape", "fw2v_batch_get_shape", "fw2v_batch_set_launch",
     "fw2v_batch_get_launch", "fw2v_batch_tune", "fw2v_batch_train", "fw2v_batch_train_epochs",
@@ -106,6 +106,8 @@ def lib() -> C.CDLL:
             "fw2v_load_corpus": (C.c_int, [H, P, I64, P, I64]),
             "fw2v_load_corpus_device": (C.c_int, [H, P, I64, P, I64]),
             "fw2v_reorder_chunks": (C.c_int, [H, P, I64]),
+            "fw2v_shuffle_chunks": (C.c_int, [H, U64]),
+            "fw2v_get_chunks": (C.c_int, [H, P]),
             "fw2v_sample_epoch": (C.c_int, [H]),
             "fw2v_epoch_sample_sizes": (C.c_int, [H, C.POINTER(I64), C.POINTER(I64)]),
             "fw2v_epoch_samples": (C.c_int, [H, P, P, P, P, P, P, P]),
@@ -272,6 +274,15 @@ class Trainer:
         chunk_off = np.ascontiguousarray(chunk_off, np.int64)
         self._check(lib().fw2v_reorder_chunks(self._h, _p(chunk_off), len(chunk_off)),
                     "reorder_chunks")
+
+    def shuffle_chunks(self, key: int):
+        """Seeded Fisher-Yates of the stored chunks on the device."""
+        self._check(lib().fw2v_shuffle_chunks(self._h, key & (2**64 - 1)), "shuffle_chunks")
+
+    def chunks(self, n: int) -> np.ndarray:
+        out = np.zeros(n, np.int64)
+        self._check(lib().fw2v_get_chunks(self._h, _p(out)), "get_chunks")
+        return out
 
     # -- epoch loop ----------------------------------------------------------
     def sample_epoch(self):

@@ -130,6 +130,17 @@ fw2v_status fw2v_load_corpus_device(fw2v_handle* h, const int32_t* stream, int64
  * epochs (no sampled epoch waiting to be trained). */
 fw2v_status fw2v_reorder_chunks(fw2v_handle* h, const int64_t* chunk_off, int64_t n_chunks);
 
+/* A seeded shuffle of the stored chunks on the device, in place of the
+ * reference's libc rand() shuffle (shuffleSentences,
+ * improved_driver_functions.cpp:283-291; -pre-shuffle / -epoch-shuffle,
+ * FULL-W2V-driver.cu:249-266, 423): Fisher-Yates from the last chunk down,
+ * chunk i swapped with j = high 64 bits of mix64(key ^ mix64(i)) * (i + 1)
+ * (mix64: the SplitMix64 finaliser).  The same key gives the same order on any
+ * device; fw2v_get_chunks reads the order back (n_chunks offsets).  Same
+ * calling rules as fw2v_reorder_chunks. */
+fw2v_status fw2v_shuffle_chunks(fw2v_handle* h, uint64_t key);
+fw2v_status fw2v_get_chunks(fw2v_handle* h, int64_t* chunk_off);
+
 /* Run the on-device batch builder for the next epoch only. */
 fw2v_status fw2v_sample_epoch(fw2v_handle* h);
 /* Sizes of the last sampled epoch: entries and kept ids summed over streams. */

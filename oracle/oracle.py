@@ -163,34 +163,40 @@ class StreamEpoch:
 
 def sample_streams(corpus: Corpus, *, threads: int, msl: int, negative: int, epochs: int,
                    alpha0: float, sample: float, table_size: int = UNIGRAM_TABLE_SIZE,
-                   runs=None, seed: int = 0):
+                   runs=None, seed: int = 0, orders=None):
     """Run the reference batch builder for every stream and epoch.
 
+    orders: optional chunk order of each epoch (the stored sentences permuted
+    between epochs, as -pre-shuffle / -epoch-shuffle do); the streams' LCG and
+    learning-rate state carry across epochs either way.
     Returns out[stream][epoch] -> StreamEpoch.
     """
     L = lib()
     stream = np.ascontiguousarray(corpus.stream, np.int32)
-    chunk_off = np.ascontiguousarray(corpus.chunk_off, np.int64)
     counts = np.ascontiguousarray(corpus.counts, np.uint32)
     p_keep = subsample_table(counts, sample, corpus.train_words) if sample > 0 else \
         np.zeros(len(counts), np.float32)
     if runs is None:
         runs = unigram_runs(counts, table_size)
     rs, rw = runs
-    cfg = SamplerCfg(_p(stream).value, len(stream), _p(chunk_off).value, len(chunk_off),
-                     _p(p_keep).value, sample, _p(rs).value, _p(rw).value, len(rw), table_size,
-                     threads, msl, negative, epochs, alpha0, corpus.train_words)
+    if orders is None:
+        orders = [corpus.chunk_off] * epochs
+    orders = [np.ascontiguousarray(o, np.int64) for o in orders]
+    cfgs = [SamplerCfg(_p(stream).value, len(stream), _p(o).value, len(o), _p(p_keep).value, sample,
+                       _p(rs).value, _p(rw).value, len(rw), table_size, threads, msl, negative, epochs,
+                       alpha0, corpus.train_words) for o in orders]
     out = []
     for s in range(threads):
         st = StreamState()
-        L.orc_stream_init(C.byref(cfg), s, C.byref(st))
+        L.orc_stream_init(C.byref(cfgs[0]), s, C.byref(st))
         st.lcg = (st.lcg + seed_offset(seed)) & (2**64 - 1)
-        a, b = C.c_int64(), C.c_int64()
-        L.orc_stream_range(C.byref(cfg), s, C.byref(a), C.byref(b))
-        cap = int(chunk_off[b.value] if b.value < len(chunk_off) else len(stream)) - \
-            int(chunk_off[a.value]) + 2
         per_epoch = []
-        for _ in range(epochs):
+        for e in range(epochs):
+            cfg, chunk_off = cfgs[e], orders[e]
+            a, b = C.c_int64(), C.c_int64()
+            L.orc_stream_range(C.byref(cfg), s, C.byref(a), C.byref(b))
+            # a chunk holds at most msl + 1 tokens (msl, or up to and including a 0)
+            cap = min(len(stream), (b.value - a.value) * (msl + 1)) + 2
             lens = np.zeros(cap + 2, np.int32)
             alphas = np.zeros(cap + 2, np.float32)
             ids = np.zeros(cap + 2, np.int32)
@@ -205,6 +211,40 @@ def sample_streams(corpus: Corpus, *, threads: int, msl: int, negative: int, epo
             per_epoch.append(StreamEpoch(lens[:n].copy(), alphas[:n].copy(), ids[:k].copy(),
                                          negs[: k * negative].copy(), int(wr.value)))
         out.append(per_epoch)
+    return out
+
+
+def libc_shuffle(chunk_off: np.ndarray) -> np.ndarray:
+    """shuffleSentences (improved_driver_functions.cpp:283-291): Fisher-Yates
+    over the stored sentence pointers with the C library's rand(), from i =
+    n-1 down to 1, j = (int)((rand() / (double)RAND_MAX) * (i + 1)) (j = i + 1,
+    when rand() returns RAND_MAX, is taken as i: the reference would index one
+    past the array).  Continues this process's rand() sequence, as the
+    reference's successive shuffles continue its own; call libc_srand(1) first
+    for the sequence of a fresh process."""
+    libc = C.CDLL(None)
+    libc.rand.restype = C.c_int
+    out = np.array(chunk_off, np.int64, copy=True)
+    n = len(out)
+    RAND_MAX = 2147483647
+    for i in range(n - 1, 0, -1):
+        j = int((libc.rand() / float(RAND_MAX)) * (i + 1))
+        j = min(j, i)
+        out[i], out[j] = out[j], out[i]
+    return out
+
+
+def libc_srand(seed: int) -> None:
+    C.CDLL(None).srand(C.c_uint(seed))
+
+
+def device_shuffle(chunk_off: np.ndarray, key: int) -> np.ndarray:
+    """The library's seeded Fisher-Yates (fw2v_shuffle_chunks): from i = n-1 down
+    to 1, j = the high 64 bits of mix64(key ^ mix64(i)) * (i + 1), swap."""
+    out = np.array(chunk_off, np.int64, copy=True)
+    for i in range(len(out) - 1, 0, -1):
+        j = (mix64(key ^ mix64(i)) * (i + 1)) >> 64
+        out[i], out[j] = out[j], out[i]
     return out
 
 

@@ -265,6 +265,44 @@ def run_shape_case(name: str):
         shutil.rmtree(tmp)
 
 
+# The reference's shuffles (-pre-shuffle, -epoch-shuffle: libc rand(), unseeded)
+SHUFFLE_CASES = [
+    ("shuffle_t2", lambda: zipf_text(17, 12000, 1200),
+     "-size 8 -window 3 -negative 4 -sample 1e-3 -iter 3 -threads 2 -min-count 2 -msl 40 -pre-shuffle "
+     "-epoch-shuffle"),
+]
+
+
+def run_shuffle_case(name: str, text: bytes, flags: list[str]):
+    """The batches of a run with both shuffles: the corpus, the flags and each
+    thread's batches in full (the case is small)."""
+    tmp = tempfile.mkdtemp(prefix="fw2v_golden_")
+    try:
+        corpus = os.path.join(tmp, "corpus.txt")
+        with open(corpus, "wb") as f:
+            f.write(text)
+        dump = os.path.join(tmp, "dump")
+        os.mkdir(dump)
+        cmd = [HARNESS, "-train", corpus, "-output", os.path.join(tmp, "out.vec"), "-debug", "0", "-binary", "1",
+               "-streams", "1", "-kernel-batch-size", "4"] + flags
+        r = subprocess.run(cmd, env=dict(os.environ, FW2V_REF_DUMP_DIR=dump), capture_output=True, check=True,
+                           text=True)
+        overall = [ln for ln in r.stdout.splitlines() if ln.startswith("Overall Words:")]
+        per = [parse_dump(os.path.join(dump, f)) for f in sorted(os.listdir(dump))]
+        arrays = {"corpus": np.frombuffer(text, np.uint8), "flags": np.array(" ".join(flags)),
+                  "overall_words": np.array(int(overall[0].split(":")[1]), np.int64),
+                  "n_threads": np.array(len(per), np.int32)}
+        for t, (lens, alphas, ids, negs) in enumerate(per):
+            arrays[f"t{t}_lens"] = lens
+            arrays[f"t{t}_alphas"] = alphas
+            arrays[f"t{t}_ids"] = ids.astype(np.int16)
+            arrays[f"t{t}_negs"] = negs.astype(np.int16)
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), **arrays)
+        print(f"{name}: overall_words={int(arrays['overall_words'])} threads={len(per)}")
+    finally:
+        shutil.rmtree(tmp)
+
+
 def main():
     if not os.path.exists(HARNESS):
         sys.exit(f"missing {HARNESS}: run `make -C oracle ref` first")
@@ -272,6 +310,8 @@ def main():
     if not only_shapes:
         for name, gen, flags in CASES:
             run_case(name, gen(), flags.split())
+        for name, gen, flags in SHUFFLE_CASES:
+            run_shuffle_case(name, gen(), flags.split())
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import shape_cases
     for name in shape_cases.CASES:

@@ -53,12 +53,15 @@ def _built():
         pytest.skip("full-w2v is not built")
 
 
+@pytest.mark.parametrize("read_threads", [1, 3, 16])
 @pytest.mark.parametrize("name", CASES)
-def test_preprocessing_files_match_reference(name, tmp_path):
+def test_preprocessing_files_match_reference(name, read_threads, tmp_path):
+    """Serial and parallel text readers (the file cut into 3 or 16 segments at
+    line starts) give the reference's vocabulary, cache and corpus files."""
     g = load(name)
     (tmp_path / "corpus.txt").write_bytes(g["text"])
     _run(["-train", "corpus.txt", "-debug", "0", "-save-vocab", "v.txt", "-save-corpus-cache", "c.txt",
-          "-save-corpus", "s.txt"] + _flags(g), tmp_path)
+          "-save-corpus", "s.txt", "-read-threads", str(read_threads)] + _flags(g), tmp_path)
     assert (tmp_path / "v.txt").read_bytes() == g["vocab_text"]
     assert (tmp_path / "c.txt").read_bytes() == g["cache_text"]
     assert _sha(tmp_path / "s.txt") == str(g["corpus_text_sha256"])
@@ -177,3 +180,18 @@ def test_jobs_manifest_trains_each_job_as_alone(tmp_path, precision):
     assert "Job 2 Words:" in out and "Overall Words Per Second:" in out
     for i in range(2):
         assert (tmp_path / f"j{i}.vec").read_bytes() == (tmp_path / f"a{i}.vec").read_bytes()
+
+
+@pytest.mark.parametrize("name", ["c1_t16", "c2cut_t64"])
+def test_parallel_reader_vocab_matches_reference_at_shape(name, tmp_path):
+    """The benchmark-shaped corpora (1M and 2M tokens) read by 8 threads: the
+    vocabulary file equals the reference program's (digest in
+    tests/golden/shape_<name>.json)."""
+    import shape_cases as S
+    from fw2v import synth
+    raw, ends, _ = S.raw_tokens(name)
+    (tmp_path / "corpus.txt").write_bytes(synth.text_of(raw, ends))
+    f = S.flags_of(name)
+    _run(["-train", "corpus.txt", "-debug", "0", "-save-vocab", "v.txt", "-read-threads", "8",
+          "-min-count", str(f["min_count"]), "-msl", str(f["msl"])], tmp_path)
+    assert _sha(tmp_path / "v.txt") == S.load(name)["vocab_sha256"]
