@@ -462,7 +462,7 @@ def run_own(args, world, rank, local):
         out["cpu_baseline"] = cpu_baseline(corpus, cfg, T)
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         del corpus, held, pairs
-        out["reference_gpu"] = reference_gpu(local)
+        out["reference_gpu"] = reference_gpu(local, args.reference_gpu, args.ref_walks_per_node)
     return out
 
 
@@ -489,14 +489,14 @@ def safe_reference_threads(corpus, cfg, epochs, cores, streams=4, batch=200):
     return 0
 
 
-def run_reference_program(binary, text, cfg, epochs, threads, streams=4, batch=200):
+def run_reference_program(binary, text, cfg, epochs, threads, streams=4, batch=200, extra=()):
     """FULL-W2V on a text corpus; (words/s, overall seconds) or a reason string."""
-    cmd = [binary, "-train", text, "-size", str(cfg["d"]), "-window", str(cfg["window"]),
+    cmd = [binary, "-train", text] + list(extra) + [ "-size", str(cfg["d"]), "-window", str(cfg["window"]),
            "-negative", str(cfg["negative"]), "-sample", str(cfg["sample"]), "-iter", str(epochs),
            "-alpha", "0.025", "-min-count", str(cfg["min_count"]), "-threads", str(threads),
            "-streams", str(streams), "-kernel-batch-size", str(batch), "-msl", "1000",
            "-debug", "0", "-no-export", "-output", os.devnull]
-    r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
     if r.returncode != 0:
         return f"reference exited {r.returncode}: {r.stderr[-300:]}"
     wps = [ln for ln in r.stdout.splitlines() if ln.startswith("Overall Words Per Second:")]
@@ -506,14 +506,27 @@ def run_reference_program(binary, text, cfg, epochs, threads, streams=4, batch=2
     return float(wps[0].split(":")[1]), (float(tim[0].split(":")[1]) if tim else None)
 
 
-def reference_gpu(local):
+def write_walk_text(corpus, path, walk_len):
+    """A walk corpus as text, one walk per line, each word its vocabulary id:
+    the reference's text front end builds the same vocabulary from it (counts,
+    ties by first occurrence) and, with -cache-eos, the same sentences."""
+    ids = corpus.host_stream()[:-1].reshape(-1, walk_len + 1)[:, :walk_len]
+    with open(path, "w") as f:
+        for s0 in range(0, len(ids), 100_000):
+            np.savetxt(f, ids[s0:s0 + 100_000], fmt="%d", delimiter=" ")
+
+
+def reference_gpu(local, which="c2", walks_per_node=1):
     """The reference's CUDA program and the plain FP32 kernel of this library on
-    the same text-scale corpus (C2: 17M tokens, V=71k after min-count 5,
-    d=128, window 8, negative 5, sample 1e-4, 5 epochs), one after the other
-    on this GPU.  Each rate is the implementation's own: the reference's
-    "Overall Words Per Second" (its clock runs from after set-up to its final
-    device sync, FULL-W2V-driver.cu:162, 324, 450); ours, words read over the
-    device time of the 5 epochs (sampler and trainer, CUDA events)."""
+    the same corpus, one after the other on this GPU.  c2: the text-scale
+    corpus (17M tokens, V=71k after min-count 5, d=128, window 8, negative 5,
+    sample 1e-4, 5 epochs).  c4: the 1M-node stochastic-block-model graph
+    with `walks_per_node` walks of 80 per node (C4 has 10), written one walk
+    per line and read with -cache-eos (d=128, window 10, sample 1e-3, 1
+    epoch).  Each rate is the implementation's own: the reference's "Overall
+    Words Per Second" (its clock runs from after set-up to its final device
+    sync, FULL-W2V-driver.cu:162, 324, 450); ours, words read over the device
+    time of the epochs (sampler and trainer, CUDA events)."""
     import torch
 
     import fw2v
@@ -521,28 +534,45 @@ def reference_gpu(local):
     binary = os.path.join(ROOT, "baseline", "_ref", "FULL-W2V")
     if not os.path.exists(binary):
         return {"unavailable": "baseline/_ref/FULL-W2V not built (make -C baseline with the reference checkout)"}
-    cfg = dict(synth.CONFIGS["c2"])
-    epochs = cfg["epochs"]
-    raw, planted, _ = synth.topic_tokens(cfg["n_tokens"], cfg["vocab"], cfg["topics"], cfg["zipf_s"], seed=1236)
-    ends = np.arange(1000, len(raw) + 1000, 1000)
-    ends[-1] = len(raw)
-    corpus = synth.build_stream(raw, ends, planted, min_count=cfg["min_count"], msl=1000)
-    cores = os.cpu_count() or 1
-    threads = safe_reference_threads(corpus, cfg, epochs, cores)
-    if threads < 1:
-        return {"unavailable": "corpus too small for the reference's launch pattern"}
+    dev = torch.device("cuda", local)
     tmp = tempfile.mkdtemp(prefix="fw2v_ref_")
+    text = os.path.join(tmp, "corpus.txt")
     try:
-        text = os.path.join(tmp, "corpus.txt")
-        with open(text, "wb") as f:
-            f.write(synth.text_of(raw, ends))
-        del raw
-        ref = run_reference_program(binary, text, cfg, epochs, threads)
+        if which == "c2":
+            cfg = dict(synth.CONFIGS["c2"])
+            raw, planted, _ = synth.topic_tokens(cfg["n_tokens"], cfg["vocab"], cfg["topics"], cfg["zipf_s"],
+                                                 seed=1236)
+            ends = np.arange(1000, len(raw) + 1000, 1000)
+            ends[-1] = len(raw)
+            corpus = synth.build_stream(raw, ends, planted, min_count=cfg["min_count"], msl=1000)
+            with open(text, "wb") as f:
+                f.write(synth.text_of(raw, ends))
+            del raw
+            extra = ()
+            workload = (f"c2: {cfg['n_tokens'] / 1e6:.0f}M-token topic corpus, V={len(corpus.counts)}, d={cfg['d']}, "
+                        f"window={cfg['window']}, negative={cfg['negative']}, sample={cfg['sample']}, msl=1000, "
+                        f"{cfg['epochs']} epochs")
+        else:
+            g = dict(synth.GRAPH_CONFIGS["c4"])
+            corpus, _ = synth.sbm_corpus_gpu(g["nodes"], g["blocks"], g["degree"], g["p_ratio"], walks_per_node,
+                                             g["walk_len"], seed=1234 + 4)
+            write_walk_text(corpus, text, g["walk_len"])
+            cfg = dict(g, min_count=1)
+            extra = ("-cache-eos",)
+            workload = (f"c4 graph ({g['nodes']} nodes, {g['blocks']} blocks), {walks_per_node} walk(s) of "
+                        f"{g['walk_len']} per node ({len(corpus.stream) - 1} tokens with </s>), V={len(corpus.counts)}, "
+                        f"d={g['d']}, window={g['window']}, negative={g['negative']}, sample={g['sample']}, "
+                        f"-cache-eos, {g['epochs']} epoch")
+        epochs = cfg["epochs"]
+        cores = os.cpu_count() or 1
+        threads = safe_reference_threads(corpus, cfg, epochs, cores)
+        if threads < 1:
+            return {"unavailable": "corpus too small for the reference's launch pattern"}
+        ref = run_reference_program(binary, text, cfg, epochs, threads, extra=extra)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     if isinstance(ref, str):
         return {"unavailable": ref}
-    dev = torch.device("cuda", local)
     T = default_streams(len(corpus.chunk_off))
     c = fw2v.default_config(layer_size=cfg["d"], window=cfg["window"], negative=cfg["negative"], epochs=epochs,
                             threads=T, msl=1000, alpha=0.025, sample=cfg["sample"])
@@ -558,9 +588,7 @@ def reference_gpu(local):
         e1.synchronize()
         secs = e0.elapsed_time(e1) / 1e3
     ours = words / secs
-    return {"workload": f"c2: {cfg['n_tokens'] / 1e6:.0f}M-token topic corpus, V={len(corpus.counts)}, d={cfg['d']}, "
-                        f"window={cfg['window']}, negative={cfg['negative']}, sample={cfg['sample']}, msl=1000, "
-                        f"{epochs} epochs; both on this GPU, one after the other",
+    return {"workload": workload + "; both on this GPU, one after the other",
             "reference": {"value": ref[0], "unit": UNIT, "overall_time_s": ref[1], "host_threads": threads,
                           "streams": 4, "kernel_batch_size": 200,
                           "program": "baseline/_ref/FULL-W2V: the reference's FULL-W2V-driver.cu and "
@@ -568,126 +596,6 @@ def reference_gpu(local):
             "fp32_plain": {"value": ours, "unit": UNIT, "device_time_s": secs, "words": int(words),
                            "sampling_streams": T, "kernel": "sgns_train_kernel, default shape"},
             "speedup": ours / ref[0]}
-
-
-def run_c5(args, world, rank, local):
-    """The batched configuration: 256 independent graph jobs (synth.c5_job_specs,
-    node counts times --scale).  Each job is generated on the device, trained
-    alone with the plain FP32 single-job kernel (timed, scored), then added to
-    one batch that trains all of them in the value's form (tuned, one CUDA
-    graph).  value = words of all jobs / the batch's device time; fp32_alone =
-    the same words / the sum of the jobs' own device times.  On N ranks the jobs
-    are partitioned by token count (fw2v.shard.assign_jobs); each rank trains
-    its share, and the words of all ranks count over the slowest rank's time."""
-    import torch
-
-    import fw2v
-    from fw2v import evaluate, synth
-    from fw2v.shard import combine_ranks, rank_share
-
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
-    all_specs = synth.c5_job_specs(scale=args.scale)
-    specs = [all_specs[j] for j in rank_share(all_specs, world, rank)]
-    prec = fw2v.BF16 if args.form.startswith("bf16") else fw2v.FP32
-    batch = fw2v.Batch(precision=prec, device=local, group_bytes=args.group_bytes)
-    labels, alone_p10, alone_ms, alone_words = [], [], 0.0, 0
-    for j, s in enumerate(specs):
-        corpus, _ = synth.sbm_corpus_gpu(s["nodes"], s["blocks"], s["degree"], s["p_ratio"], s["walks_per_node"],
-                                         s["walk_len"], seed=s["seed"])
-        T = default_streams(len(corpus.chunk_off))
-        cfg = fw2v.default_config(layer_size=s["d"], window=s["window"], negative=s["negative"], epochs=s["epochs"],
-                                  threads=T, msl=1000, alpha=0.025, sample=s["sample"], seed=s["seed"])
-        if not args.no_compare:
-            with fw2v.Trainer(cfg) as t:
-                t.set_vocab(corpus.counts, corpus.train_words)
-                t.load_corpus(corpus.stream, corpus.chunk_off)
-                ts = torch.cuda.ExternalStream(t.stream_handle(), device=dev)
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(ts)
-                alone_words += t.train()
-                e1.record(ts)
-                e1.synchronize()
-                alone_ms += e0.elapsed_time(e1)
-                alone_p10.append(evaluate.precision_at_10(t.syn0(), corpus.label, corpus.counts,
-                                                          purity=corpus.purity, device=dev)[0])
-        batch.add_job(cfg, corpus.counts, corpus.train_words, corpus.stream, corpus.chunk_off)
-        labels.append((corpus.label, corpus.counts, corpus.purity))
-        del corpus
-    tuned = batch.tune()
-    barrier(world)
-    with ClockSampler(local) as clk:
-        torch.cuda.synchronize(dev)
-        st = batch.train()
-        torch.cuda.synchronize(dev)
-    barrier(world)
-    tot = combine_ranks(st.words_read, st.ms / 1e3, alone_words, alone_ms / 1e3, device=dev)
-    batch_s, words_all, value = tot["seconds"], tot["words"], tot["value"]
-    p10 = [evaluate.precision_at_10(batch.syn0(j), *labels[j][:2], purity=labels[j][2], device=dev)[0]
-           for j in range(len(specs))]
-    batch.close()
-    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": 1, "warmup": 0,
-           "ms_per_step": batch_s * 1e3, "higher_is_better": True, "scaling": "strong" if world > 1 else "weak",
-           "vs_baseline": None,
-           "dtype": "bf16-tables/f32-math" if prec == fw2v.BF16 else "f32",
-           "data": "synthetic (seeded random walks on 256 stochastic block models, generated in-process)",
-           "config": {"workload": f"c5: {len(all_specs)} graph jobs, {words_all / 1e9:.2f}B tokens, one batch per "
-                                  f"rank; form {args.form}", "form": args.form, "jobs": len(all_specs),
-                      "jobs_this_rank": len(specs), "scale": args.scale,
-                      "parallelism": f"jobs partitioned over {world} ranks" if world > 1 else "single GPU",
-                      "rounds": st.rounds, "group_bytes": args.group_bytes, "tuning": tuned},
-           "precision_at_10": {"mean": float(np.nanmean(p10)), "min": float(np.nanmin(p10))},
-           "gpu_launches": 5 * st.rounds}
-    if alone_p10:
-        diff = np.array(p10) - np.array(alone_p10)
-        alone_value = tot["alone_value"]
-        out["fp32_alone"] = {"form": "each job alone, fp32 single-job kernel", "value": alone_value,
-                             "unit": UNIT, "speedup": value / alone_value,
-                             "precision_at_10_mean": float(np.nanmean(alone_p10)),
-                             "p10_diff_mean": float(np.nanmean(diff)), "p10_diff_min": float(np.nanmin(diff)),
-                             "jobs_within_1_point": int(np.sum(diff >= -0.01))}
-    clocks = clk.summary()
-    if clocks:
-        out["clocks"] = clocks
-    return out
-
-
-def run_reference(args, world, rank):
-    """The reference program (oracle/_ref/FULL-W2V) on the same corpus, or the
-    CPU port where it cannot run."""
-    from fw2v import synth
-    from oracle import oracle as O
-
-    if world > 1 and rank != 0:
-        return None
-    if args.config == "c5":
-        return {"impl": "reference", "unavailable": "the reference trains one corpus per process; the batched "
-                                                    "configuration has no reference form (use --config c3)"}
-    corpus, _, cfg = make_corpus(args)
-    T_stream = args.streams or default_streams(len(corpus.chunk_off))
-    cores = os.cpu_count() or 1
-    binary = os.path.join(ROOT, "baseline", "_ref", "FULL-W2V")
-    reason = None
-    if args.config not in ("c1", "c2"):
-        reason = f"{args.config} is generated on the device and is not written as text for the reference program"
-    elif cfg["d"] > 256 or cfg["d"] % 32:
-        reason = f"reference kernel unsupported at d={cfg['d']} (shared-memory overlap / partial warp)"
-    elif not os.path.exists(binary):
-        reason = "baseline/_ref/FULL-W2V not built"
-    if reason is None:
-        res = reference_program(args, corpus, cfg, binary, cores)
-        if isinstance(res, dict):
-            return res
-        reason = res
-    base = cpu_baseline(corpus, cfg, T_stream)
-    base["sample"] += f"; reference program not run: {reason}"
-    return {"metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "impl": "reference",
-            "config": {"workload": args.config}, "cpu_baseline": base,
-            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
 
 
 def reference_program(args, corpus, cfg, binary, cores):
@@ -758,7 +666,10 @@ def main():
                     help="batched forms: table bytes per group of interleaved jobs (0: half of L2, -1: one group)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true",
-                    help="skip timing the reference's CUDA program against the plain FP32 kernel (C2)")
+                    help="skip timing the reference's CUDA program against the plain FP32 kernel")
+    ap.add_argument("--reference-gpu", default="c2", choices=["c2", "c4"],
+                    help="corpus of that comparison: c2 (text scale) or c4 (the 1M-node walk graph)")
+    ap.add_argument("--ref-walks-per-node", type=int, default=1, help="c4 comparison: walks per node (C4: 10)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
