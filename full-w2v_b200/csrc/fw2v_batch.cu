@@ -558,7 +558,6 @@ fw2v_status check_error_flag(fw2v_batch* b, const char* what) {
   BCK(b, cudaMemcpy(&flag, b->error_flag, sizeof(int), cudaMemcpyDeviceToHost));
   if (flag) {
     BCK(b, cudaMemset(b->error_flag, 0, sizeof(int)));
-    if (flag == 2) return bfail(b, FW2V_ERR_CUDA, "%s: a bulk row copy did not complete in time", what);
     return bfail(b, FW2V_ERR_BOUNDS, "%s: an id outside [0, V), a read past a token stream or a full buffer", what);
   }
   return FW2V_OK;
