@@ -422,9 +422,10 @@ __device__ __forceinline__ void row_load_global(Row<VEC, NV>& r, const bf16_t* r
 // no other writer touched the row since the load, the stored value becomes s
 // exactly.  Concurrent writers never lose each other's updates.
 __device__ __forceinline__ uint32_t sr_increment2(float a0, float b0, float a1, float b1, uint32_t r32) {
-  const float x0 = __fsub_rn(bf16_stochastic_value(a0, r32 & 0xFFFFu), b0);
-  const float x1 = __fsub_rn(bf16_stochastic_value(a1, r32 >> 16), b1);
-  const __nv_bfloat162 v = __floats2bfloat162_rn(x0, x1);  // x0 in the low half (lower address)
+  // s - b for both elements with one packed FP32x2 add (s + (-b), exact as s - b)
+  const float2 x = __fadd2_rn(make_float2(bf16_stochastic_value(a0, r32 & 0xFFFFu), bf16_stochastic_value(a1, r32 >> 16)),
+                              make_float2(-b0, -b1));
+  const __nv_bfloat162 v = __floats2bfloat162_rn(x.x, x.y);  // element 0 in the low half (lower address)
   return *reinterpret_cast<const uint32_t*>(&v);
 }
 
@@ -477,10 +478,12 @@ __device__ __forceinline__ void row_add_delta(float* row, const Row<VEC, NV>& a,
   row_add_delta(row, a, b, lane, d);
 }
 
-// Lane partial of a dot product with the packed FP32x2 FMA of sm_100 (two
-// IEEE single-rounding FMAs per instruction): elements j and j+1 of every
-// vector (j even) go to two running sums, "even" and "odd", each a product
-// then FMAs in vector order; the lane's partial is even + odd.
+// Lane partial of a dot product as two independent running sums, "even" and
+// "odd" (elements j and j+1 of every vector, j even), each a product then
+// FMAs in vector order, in sm_100's packed FP32x2 FMA (two IEEE
+// single-rounding FMAs per instruction); the lane's partial is even + odd.
+// Two chains halve the dependent latency of the dot, which sits on the
+// critical path of every pipeline step.
 template <int VEC, int NV>
 __device__ __forceinline__ float row_dot(const Row<VEC, NV>& a, const Row<VEC, NV>& b) {
   float2 p = __fmul2_rn(make_float2(a.x[0][0], a.x[0][1]), make_float2(b.x[0][0], b.x[0][1]));
@@ -499,23 +502,18 @@ __device__ __forceinline__ float warp_sum(float p) {
   return p;
 }
 
-// v += g*o and o += g*v_old, elementwise with single-rounding FMAs, two
-// elements per packed FP32x2 FMA.
+// v += g*o and o += g*v_old, elementwise with single-rounding FMAs.  (Scalar
+// FMAs issue to both FP32 pipes; the packed FP32x2 form, which runs on one,
+// measured 4% slower here.)
 template <int VEC, int NV>
 __device__ __forceinline__ void row_update(Row<VEC, NV>& v, Row<VEC, NV>& o, float g) {
-  const float2 g2 = make_float2(g, g);
 #pragma unroll
   for (int i = 0; i < NV; i++)
 #pragma unroll
-    for (int j = 0; j < VEC; j += 2) {
-      const float2 vo = make_float2(v.x[i][j], v.x[i][j + 1]);
-      const float2 oo = make_float2(o.x[i][j], o.x[i][j + 1]);
-      const float2 vn = __ffma2_rn(g2, oo, vo);
-      const float2 on = __ffma2_rn(g2, vo, oo);
-      v.x[i][j] = vn.x;
-      v.x[i][j + 1] = vn.y;
-      o.x[i][j] = on.x;
-      o.x[i][j + 1] = on.y;
+    for (int j = 0; j < VEC; j++) {
+      const float vo = v.x[i][j];
+      v.x[i][j] = __fmaf_rn(g, o.x[i][j], vo);
+      o.x[i][j] = __fmaf_rn(g, vo, o.x[i][j]);
     }
 }
 
@@ -933,15 +931,18 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
           // A row copied before the previous group's write-back of the same
           // target is fetched again (after this lane's own reduction, in
           // program order).
-          bool stale_any = false;
-          for (int k = 0; k < nt; k++) {
-            const int tk = __shfl_sync(kFull, my_t, k);
-            bool stale = false;
-            for (int j = 0; j < R; j++) stale |= __shfl_sync(kFull, t_prev, j) == tk;
-            if (stale) cp_row(cur_b + (uint32_t)k * srow_bytes, syn1neg + (int64_t)tk * P, lm, d);
-            stale_any |= stale;
-          }
-          if (stale_any) {
+          // Lane k < nt compares its target with the previous group's.
+          bool stale = false;
+#pragma unroll
+          for (int j = 0; j < R; j++) stale |= __shfl_sync(kFull, t_prev, j) == my_t;
+          unsigned stale_mask = __ballot_sync(kFull, stale && lane < nt);
+          if (stale_mask) {
+            while (stale_mask) {
+              const int k = __ffs(stale_mask) - 1;
+              stale_mask &= stale_mask - 1;
+              const int tk = __shfl_sync(kFull, my_t, k);
+              cp_row(cur_b + (uint32_t)k * srow_bytes, syn1neg + (int64_t)tk * P, lm, d);
+            }
             cp_async_commit();
             cp_async_wait();
           }
@@ -963,9 +964,12 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
         }
         if (!__any_sync(kFull, dup)) {
           // ---- pipelined sweeps of nt targets ----
+          int tks[R];  // the group's target ids, on every lane
+#pragma unroll
+          for (int k = 0; k < R; k++) tks[k] = __shfl_sync(kFull, my_t, k);
 #pragma unroll
           for (int k = 0; k < R; k++) {
-            const int tk = __shfl_sync(kFull, my_t, k);
+            const int tk = tks[k];
             if (k < nt) {
               if (pre) {
                 lds_staged<T>(o[k], cur_b + (uint32_t)k * srow_bytes, lm);
@@ -1003,9 +1007,15 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
                 const float xs = transpose_reduce<RP>(x, lane);
                 const bool act = (unsigned)(ts - my_stage) < my_span;
                 const float g = act ? gradient<SIG>(xs, my_positive, alpha, table) : 0.0f;
+                // every lane needs every stage's g; with two stages the other
+                // half-warp holds the other one
+                float g_other = 0.0f;
+                if constexpr (RP == 2) g_other = __shfl_xor_sync(kFull, g, 16);
                 static_for<R>([&](auto kc) {
                   constexpr int k = decltype(kc)::value;
-                  const float gk = __shfl_sync(kFull, g, lane_of_stage<RP>(k));
+                  float gk;
+                  if constexpr (RP == 2) gk = (my_stage == k) ? g : g_other;
+                  else gk = __shfl_sync(kFull, g, lane_of_stage<RP>(k));
                   row_update(v[(u - k + R) % R], o[k], gk);
                 });
                 constexpr int out = (u + 1) % R;
@@ -1016,7 +1026,7 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
           }
 #pragma unroll
           for (int k = 0; k < R; k++) {
-            const int tk = __shfl_sync(kFull, my_t, k);
+            const int tk = tks[k];
             if (k < nt) {
               Row<VEC, NV> o0;
               lds_staged<T>(o0, (pre ? cur_b : o0_b) + (uint32_t)k * srow_bytes, lm);
