@@ -598,6 +598,126 @@ def reference_gpu(local, which="c2", walks_per_node=1):
             "speedup": ours / ref[0]}
 
 
+def run_c5(args, world, rank, local):
+    """The batched configuration: 256 independent graph jobs (synth.c5_job_specs,
+    node counts times --scale).  Each job is generated on the device, trained
+    alone with the plain FP32 single-job kernel (timed, scored), then added to
+    one batch that trains all of them in the value's form (tuned, one CUDA
+    graph).  value = words of all jobs / the batch's device time; fp32_alone =
+    the same words / the sum of the jobs' own device times.  On N ranks the jobs
+    are partitioned by token count (fw2v.shard.assign_jobs); each rank trains
+    its share, and the words of all ranks count over the slowest rank's time."""
+    import torch
+
+    import fw2v
+    from fw2v import evaluate, synth
+    from fw2v.shard import combine_ranks, rank_share
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    all_specs = synth.c5_job_specs(scale=args.scale)
+    specs = [all_specs[j] for j in rank_share(all_specs, world, rank)]
+    prec = fw2v.BF16 if args.form.startswith("bf16") else fw2v.FP32
+    batch = fw2v.Batch(precision=prec, device=local, group_bytes=args.group_bytes)
+    labels, alone_p10, alone_ms, alone_words = [], [], 0.0, 0
+    for j, s in enumerate(specs):
+        corpus, _ = synth.sbm_corpus_gpu(s["nodes"], s["blocks"], s["degree"], s["p_ratio"], s["walks_per_node"],
+                                         s["walk_len"], seed=s["seed"])
+        T = default_streams(len(corpus.chunk_off))
+        cfg = fw2v.default_config(layer_size=s["d"], window=s["window"], negative=s["negative"], epochs=s["epochs"],
+                                  threads=T, msl=1000, alpha=0.025, sample=s["sample"], seed=s["seed"])
+        if not args.no_compare:
+            with fw2v.Trainer(cfg) as t:
+                t.set_vocab(corpus.counts, corpus.train_words)
+                t.load_corpus(corpus.stream, corpus.chunk_off)
+                ts = torch.cuda.ExternalStream(t.stream_handle(), device=dev)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(ts)
+                alone_words += t.train()
+                e1.record(ts)
+                e1.synchronize()
+                alone_ms += e0.elapsed_time(e1)
+                alone_p10.append(evaluate.precision_at_10(t.syn0(), corpus.label, corpus.counts,
+                                                          purity=corpus.purity, device=dev)[0])
+        batch.add_job(cfg, corpus.counts, corpus.train_words, corpus.stream, corpus.chunk_off)
+        labels.append((corpus.label, corpus.counts, corpus.purity))
+        del corpus
+    tuned = batch.tune()
+    barrier(world)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize(dev)
+        st = batch.train()
+        torch.cuda.synchronize(dev)
+    barrier(world)
+    tot = combine_ranks(st.words_read, st.ms / 1e3, alone_words, alone_ms / 1e3, device=dev)
+    batch_s, words_all, value = tot["seconds"], tot["words"], tot["value"]
+    p10 = [evaluate.precision_at_10(batch.syn0(j), *labels[j][:2], purity=labels[j][2], device=dev)[0]
+           for j in range(len(specs))]
+    batch.close()
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": 1, "warmup": 0,
+           "ms_per_step": batch_s * 1e3, "higher_is_better": True, "scaling": "strong" if world > 1 else "weak",
+           "vs_baseline": None,
+           "dtype": "bf16-tables/f32-math" if prec == fw2v.BF16 else "f32",
+           "data": "synthetic (seeded random walks on 256 stochastic block models, generated in-process)",
+           "config": {"workload": f"c5: {len(all_specs)} graph jobs, {words_all / 1e9:.2f}B tokens, one batch per "
+                                  f"rank; form {args.form}", "form": args.form, "jobs": len(all_specs),
+                      "jobs_this_rank": len(specs), "scale": args.scale,
+                      "parallelism": f"jobs partitioned over {world} ranks" if world > 1 else "single GPU",
+                      "rounds": st.rounds, "group_bytes": args.group_bytes, "tuning": tuned},
+           "precision_at_10": {"mean": float(np.nanmean(p10)), "min": float(np.nanmin(p10))},
+           "gpu_launches": 5 * st.rounds}
+    if alone_p10:
+        diff = np.array(p10) - np.array(alone_p10)
+        alone_value = tot["alone_value"]
+        out["fp32_alone"] = {"form": "each job alone, fp32 single-job kernel", "value": alone_value,
+                             "unit": UNIT, "speedup": value / alone_value,
+                             "precision_at_10_mean": float(np.nanmean(alone_p10)),
+                             "p10_diff_mean": float(np.nanmean(diff)), "p10_diff_min": float(np.nanmin(diff)),
+                             "jobs_within_1_point": int(np.sum(diff >= -0.01))}
+    clocks = clk.summary()
+    if clocks:
+        out["clocks"] = clocks
+    return out
+
+
+def run_reference(args, world, rank):
+    """The reference program (oracle/_ref/FULL-W2V) on the same corpus, or the
+    CPU port where it cannot run."""
+    from fw2v import synth
+    from oracle import oracle as O
+
+    if world > 1 and rank != 0:
+        return None
+    if args.config == "c5":
+        return {"impl": "reference", "unavailable": "the reference trains one corpus per process; the batched "
+                                                    "configuration has no reference form (use --config c3)"}
+    corpus, _, cfg = make_corpus(args)
+    T_stream = args.streams or default_streams(len(corpus.chunk_off))
+    cores = os.cpu_count() or 1
+    binary = os.path.join(ROOT, "baseline", "_ref", "FULL-W2V")
+    reason = None
+    if args.config not in ("c1", "c2"):
+        reason = f"{args.config} is generated on the device and is not written as text for the reference program"
+    elif cfg["d"] > 256 or cfg["d"] % 32:
+        reason = f"reference kernel unsupported at d={cfg['d']} (shared-memory overlap / partial warp)"
+    elif not os.path.exists(binary):
+        reason = "baseline/_ref/FULL-W2V not built"
+    if reason is None:
+        res = reference_program(args, corpus, cfg, binary, cores)
+        if isinstance(res, dict):
+            return res
+        reason = res
+    base = cpu_baseline(corpus, cfg, T_stream)
+    base["sample"] += f"; reference program not run: {reason}"
+    return {"metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": args.config}, "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
 def reference_program(args, corpus, cfg, binary, cores):
     """FULL-W2V on the workload's corpus written as text, with host threads
     under which every launch reads only buffers it has filled
