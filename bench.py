@@ -220,23 +220,51 @@ def job_config(args, cfg, T, epochs, precision):
                                threads=T, msl=1000, alpha=0.025, sample=cfg["sample"], precision=precision)
 
 
-def timed_epochs(args, world, dev, run_epoch, flush, stream):
-    """W untimed epochs, then K timed ones bracketed by barrier + synchronize;
-    run_epoch() -> (words read, words kept, device ms, kernel launches)."""
+def timed_epochs(args, world, dev, run_epochs, flush, stream, back_to_back):
+    """W untimed epochs, then K timed ones bracketed by barrier + synchronize.
+    run_epochs(n) trains n epochs -> (words read, words kept, device ms,
+    kernel launches, training-kernel ms, training-kernel launches).
+    back_to_back: the K epochs run as one call, so that every epoch's
+    sampling overlaps the training before it as in a real run (inputs larger
+    than L2); otherwise one call per epoch with L2 flushed (untimed) before
+    each."""
     import torch
     for _ in range(args.warmup):
-        run_epoch()
+        run_epochs(1)
     barrier(world)
     torch.cuda.synchronize(dev)
     res = []
-    for i in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(i & 0xFF)  # L2 flush, not timed
-        torch.cuda.synchronize(dev)
-        res.append(run_epoch())
+    if back_to_back:
+        res.append(run_epochs(args.steps))
+    else:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(i & 0xFF)  # L2 flush, not timed
+            torch.cuda.synchronize(dev)
+            res.append(run_epochs(1))
     torch.cuda.synchronize(dev)
     barrier(world)
     return res
+
+
+def single_job_epochs(tr, n, dev, tstream):
+    """n epochs of a single-job handle timed on the device: an event before
+    the first, and one recorded once the device is idle after the last (the
+    handle samples the next epoch on a second stream while one trains)."""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(tstream)
+    words = kept = 0
+    train_ms = 0.0
+    for _ in range(n):
+        st = tr.train_epoch()
+        words += st.words_read
+        kept += st.words_kept
+        train_ms += st.train_ms
+    torch.cuda.synchronize(dev)
+    e1.record(tstream)
+    e1.synchronize()
+    return words, kept, e0.elapsed_time(e1), 4 * n, train_ms, n
 
 
 def heldout(tr_cls, corpus, cfg, pairs, syn0, syn1):
@@ -266,6 +294,8 @@ def run_own(args, world, rank, local):
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
     form = args.form
+    # tables and corpus far larger than L2 (C3, C4): time the epochs back to back
+    back_to_back = args.config in ("c3", "c4") and not args.per_epoch
     bf16 = form.startswith("bf16")
     prec = fw2v.BF16 if bf16 else fw2v.FP32
     pairs = None
@@ -288,13 +318,12 @@ def run_own(args, world, rank, local):
             else:
                 tuned = b.tune(cache=tune_cache)
 
-            def run_epoch():
+            def run_epochs(n):
                 # per round: sampler, negatives, entry prefix, job bookkeeping, trainer
-                st = b.train_epochs(1)
-                return st.words_read, st.words_kept, st.ms, 5 * st.rounds, st.train_ms, st.train_launches
+                st = b.train_epochs(n)
+                return st.words_read, st.words_kept, st.ms, 5 * st.rounds * n, st.train_ms, st.train_launches
 
-            res = timed_epochs(args, world, dev, run_epoch, flush, stream)
-            syn0, syn1 = b.syn0(0), b.syn1neg(0)
+            res = timed_epochs(args, world, dev, run_epochs, flush, stream, back_to_back)
             shape = b.shape(0)
             b.close()
         else:
@@ -303,29 +332,24 @@ def run_own(args, world, rank, local):
             tr.load_corpus(corpus.stream, corpus.chunk_off)
             tstream = torch.cuda.ExternalStream(tr.stream_handle(), device=dev)
 
-            # device time of an epoch: events on the trainer's stream around it;
             # per epoch: sampler, negatives, entry prefix, trainer
-            def run_epoch_timed():
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(tstream)
-                st = tr.train_epoch()
-                e1.record(tstream)
-                e1.synchronize()
-                return st.words_read, st.words_kept, e0.elapsed_time(e1), 4, st.train_ms, 1
-
-            res = timed_epochs(args, world, dev, run_epoch_timed, flush, stream)
-            syn0, syn1 = tr.syn0(), tr.syn1neg()
+            res = timed_epochs(args, world, dev, lambda n: single_job_epochs(tr, n, dev, tstream), flush, stream,
+                               back_to_back)
             shape = None
             tr.close()
     words = sum(r[0] for r in res)  # res: (read, kept, epoch ms, launches, train ms, train launches)
     kept = sum(r[1] for r in res)
     total_s = max_over_ranks(world, sum(r[2] for r in res) / 1e3)
     value = sum_over_ranks(world, float(words)) / total_s
-    loss = heldout(fw2v.Trainer, corpus, cfg, pairs, syn0, syn1) if pairs is not None else None
-    p10 = None
-    if corpus.purity is not None:
-        p10, _ = evaluate.precision_at_10(syn0, corpus.label, corpus.counts, purity=corpus.purity, device=dev)
-    del syn0, syn1
+
+    def quality(s0, s1):
+        """Held-out loss and precision@10 of tables trained for exactly one
+        epoch (the configurations' epoch count)."""
+        loss = heldout(fw2v.Trainer, corpus, cfg, pairs, s0, s1) if pairs is not None else None
+        p10 = None
+        if corpus.purity is not None:
+            p10, _ = evaluate.precision_at_10(s0, corpus.label, corpus.counts, purity=corpus.purity, device=dev)
+        return loss, p10
 
     # e2e: through the public API from pinned host buffers, every step
     pinned = torch.empty(len(corpus.stream), dtype=torch.int32, pin_memory=True)
@@ -352,13 +376,18 @@ def run_own(args, world, rank, local):
                     eb.tune(cache=tune_cache)  # the shapes chosen above, from the cache
                 st = eb.train_epochs(1)
                 e2e_words += st.words_read
+                e2e_s += time.perf_counter() - t0
+                if i == 0:  # a fresh one-epoch model of the value's form: its quality (untimed)
+                    loss, p10 = quality(eb.syn0(0), eb.syn1neg(0))
         else:
             with fw2v.Trainer(job_config(args, cfg, T, 1, prec)) as et:
                 et.set_vocab(corpus.counts, corpus.train_words)
                 et.load_corpus(host_stream, host_chunks)
                 et.sample_epoch()
                 e2e_words += et.train_sampled().words_read
-        e2e_s += time.perf_counter() - t0
+                e2e_s += time.perf_counter() - t0
+                if i == 0:
+                    loss, p10 = quality(et.syn0(), et.syn1neg())
     e2e_s = max_over_ranks(world, e2e_s)
     e2e_value = sum_over_ranks(world, float(e2e_words)) / e2e_s
     h2d = 4 * len(corpus.stream) + 8 * len(corpus.chunk_off) + corpus.counts.nbytes
@@ -367,31 +396,33 @@ def run_own(args, world, rank, local):
     # the plain FP32 kernel on the same workload, for the form's speed-up
     compare = None
     if form != "fp32" and not args.no_compare:
-        tr = fw2v.Trainer(job_config(args, cfg, T, 1 + min(args.steps, 2), fw2v.FP32))
-        tr.set_vocab(corpus.counts, corpus.train_words)
-        tr.load_corpus(corpus.stream, corpus.chunk_off)
-        tstream = torch.cuda.ExternalStream(tr.stream_handle(), device=dev)
-        tr.train_epoch()
-        ms, cw = 0.0, 0
-        for i in range(min(args.steps, 2)):
-            with torch.cuda.stream(stream):
-                flush.fill_(i & 0xFF)
+        # speed: one untimed epoch, then min(K, 2) timed the same way as the value's
+        n_cmp = min(args.steps, 2)
+        with fw2v.Trainer(job_config(args, cfg, T, 1 + n_cmp, fw2v.FP32)) as tr:
+            tr.set_vocab(corpus.counts, corpus.train_words)
+            tr.load_corpus(corpus.stream, corpus.chunk_off)
+            tstream = torch.cuda.ExternalStream(tr.stream_handle(), device=dev)
+            tr.train_epoch()
             torch.cuda.synchronize(dev)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(tstream)
-            cw += tr.train_epoch().words_read
-            e1.record(tstream)
-            e1.synchronize()
-            ms += e0.elapsed_time(e1)
+            if back_to_back:
+                cres = [single_job_epochs(tr, n_cmp, dev, tstream)]
+            else:
+                cres = []
+                for i in range(n_cmp):
+                    with torch.cuda.stream(stream):
+                        flush.fill_(i & 0xFF)
+                    torch.cuda.synchronize(dev)
+                    cres.append(single_job_epochs(tr, 1, dev, tstream))
+        cw, ms = sum(r[0] for r in cres), sum(r[2] for r in cres)
         cval = sum_over_ranks(world, float(cw)) / max_over_ranks(world, ms / 1e3)
-        cs0 = tr.syn0()
-        closs = heldout(fw2v.Trainer, corpus, cfg, pairs, cs0, tr.syn1neg()) if pairs is not None else None
-        cp10 = None
-        if corpus.purity is not None:
-            cp10, _ = evaluate.precision_at_10(cs0, corpus.label, corpus.counts, purity=corpus.purity, device=dev)
-        tr.close()
+        # quality: a fresh one-epoch FP32 model
+        with fw2v.Trainer(job_config(args, cfg, T, 1, fw2v.FP32)) as tq:
+            tq.set_vocab(corpus.counts, corpus.train_words)
+            tq.load_corpus(corpus.stream, corpus.chunk_off)
+            tq.train_epoch()
+            closs, cp10 = quality(tq.syn0(), tq.syn1neg())
         compare = {"form": "fp32 (single-job kernel, untuned)", "value": cval, "unit": UNIT,
-                   "epochs_timed": min(args.steps, 2), "heldout_loss": closs, "precision_at_10": cp10,
+                   "epochs_timed": n_cmp, "heldout_loss": closs, "precision_at_10": cp10,
                    "speedup": value / cval,
                    "heldout_loss_rel_diff": (loss - closs) / closs if loss is not None and closs else None}
 
@@ -431,8 +462,9 @@ def run_own(args, world, rank, local):
                    "layer_size": d, "window": W, "negative": K, "streams": T, "shape": shape,
                    "tuning": tuned,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": "flushed between steps (256 MB write, untimed); tables exceed L2"
-                         if args.config == "c3" else "flushed between steps (256 MB write, untimed)"},
+                   "l2": ("tables and corpus exceed L2; the K timed epochs run back to back in one call"
+                          if back_to_back else "flushed between steps (256 MB write, untimed)"),
+                   "quality": "held-out loss and precision@10 of fresh one-epoch models of each form"},
         "heldout_loss": loss,
         "precision_at_10": p10,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
@@ -785,6 +817,8 @@ def main():
     ap.add_argument("--group-bytes", type=int, default=0,
                     help="batched forms: table bytes per group of interleaved jobs (0: half of L2, -1: one group)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--per-epoch", action="store_true",
+                    help="c3/c4: time one call per epoch with L2 flushed between them instead of back to back")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's CUDA program against the plain FP32 kernel")
     ap.add_argument("--reference-gpu", default="c2", choices=["c2", "c4"],
