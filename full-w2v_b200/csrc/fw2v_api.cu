@@ -150,6 +150,7 @@ fw2v_status check_flag(fw2v_handle* h, const char* what) {
   CK(h, cudaStreamSynchronize(h->stream));
   if (flag) {
     CK(h, cudaMemsetAsync(h->error_flag, 0, sizeof(int), h->stream));
+    if (flag == 2) return fail(h, FW2V_ERR_CUDA, "%s: a bulk row copy did not complete in time", what);
     return fail(h, FW2V_ERR_BOUNDS, "%s: an id outside [0, V) or a read past the token stream", what);
   }
   return FW2V_OK;

@@ -76,7 +76,9 @@ struct BatchJob {
   std::vector<int64_t> sbase;  // threads + 1: readable-token prefix of its streams
   int64_t gfirst = 0;          // global number of its stream 0
   int lane_vec = 4, lane_nv = 1, stages = 6;
-  int prefetch = 0;  // target rows of each group copied while the previous group trains
+  // bit 0: target rows of each group copied while the previous group trains;
+  // bit 1: context rows staged by bulk copies
+  int prefetch = 0;
   int family() const { return batch_family(lane_nv, stages); }
 };
 
@@ -254,7 +256,7 @@ void free_plan(fw2v_batch* b) {
 }
 
 int64_t shape_smem_floats(const BatchJob& j, int elem) {
-  return warp_smem_bytes(2 * j.cfg.window + 1, j.stages, j.prefetch != 0, j.pitch, elem) / 4;
+  return warp_smem_bytes(2 * j.cfg.window + 1, j.stages, (j.prefetch & 1) != 0, j.pitch, elem) / 4;
 }
 int64_t shape_scratch_elems(const BatchJob& j) { return (int64_t)(2 * j.cfg.window + 1) * j.pitch; }
 
@@ -318,7 +320,8 @@ TrainParams train_params(const fw2v_batch* b, const BatchJob& j, const RoundBuf&
   p.lane_vec = j.lane_vec;
   p.lane_nv = j.lane_nv;
   p.stages = j.stages;
-  p.prefetch = j.prefetch;
+  p.prefetch = j.prefetch & 1;
+  p.bulk = (j.prefetch >> 1) & 1;
   return p;
 }
 
@@ -558,6 +561,7 @@ fw2v_status check_error_flag(fw2v_batch* b, const char* what) {
   BCK(b, cudaMemcpy(&flag, b->error_flag, sizeof(int), cudaMemcpyDeviceToHost));
   if (flag) {
     BCK(b, cudaMemset(b->error_flag, 0, sizeof(int)));
+    if (flag == 2) return bfail(b, FW2V_ERR_CUDA, "%s: a bulk row copy did not complete in time", what);
     return bfail(b, FW2V_ERR_BOUNDS, "%s: an id outside [0, V), a read past a token stream or a full buffer", what);
   }
   return FW2V_OK;
@@ -834,7 +838,8 @@ fw2v_status fw2v_batch_set_shape(fw2v_batch* b, int32_t job, int32_t lane_vec, i
   j.lane_vec = lane_vec;
   j.lane_nv = lane_nv;
   j.stages = stages;
-  j.prefetch = prefetch != 0;
+  if (prefetch < 0 || prefetch > 3) return bfail(b, FW2V_ERR_ARGUMENT, "prefetch bits are 0..3");
+  j.prefetch = prefetch;
   return FW2V_OK;
 }
 
@@ -1129,7 +1134,7 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
     int best_vec = def_vec, best_nv = def_nv, best_st = def_st, best_pre = 0;
     for (int vec : {2, 4}) {
       for (int st : kBatchStages) {
-        for (int pre : {0, 1}) {
+        for (int pre : {0, 1, 2, 3}) {
           if (result != FW2V_OK || !valid_shape(d_max, vec, def_nv, st)) continue;
           for (int j : members[c]) {
             b->jobs[j].lane_vec = vec;

@@ -74,39 +74,36 @@ __host__ __device__ constexpr int batch_family(int nv, int stages) {
 // Rows of three vectors per lane stop at 4 stages: their 6-stage body does not
 // fit the register file.
 template <typename T, int VEC, int NV>
-__device__ __forceinline__ void batch_stages(const TrainParams& p, const Sentence& sn, float* ring, T* orig,
-                                             const float* table, int lane) {
+__device__ __forceinline__ bool batch_stages(const TrainParams& p, const Sentence& sn, float* ring, T* orig,
+                                             const float* table, int lane, uint32_t bar, uint32_t& phase) {
   switch (p.stages) {
-    case 2: train_sentence<T, VEC, NV, 2, 0>(p, sn, ring, orig, table, lane); break;
-    case 3: train_sentence<T, VEC, NV, 3, 0>(p, sn, ring, orig, table, lane); break;
-    case 4: train_sentence<T, VEC, NV, 4, 0>(p, sn, ring, orig, table, lane); break;
+    case 2: return train_sentence<T, VEC, NV, 2, 0>(p, sn, ring, orig, table, lane, bar, phase);
+    case 3: return train_sentence<T, VEC, NV, 3, 0>(p, sn, ring, orig, table, lane, bar, phase);
+    case 4: return train_sentence<T, VEC, NV, 4, 0>(p, sn, ring, orig, table, lane, bar, phase);
     default:
-      if constexpr (NV < 3) train_sentence<T, VEC, NV, 6, 0>(p, sn, ring, orig, table, lane);
-      break;
+      if constexpr (NV < 3) return train_sentence<T, VEC, NV, 6, 0>(p, sn, ring, orig, table, lane, bar, phase);
+      return true;
   }
 }
 
+// False if the sentence stopped on a bulk copy that did not complete.
 template <typename T, int FAMILY>
-__device__ __forceinline__ void batch_dispatch(const TrainParams& p, const Sentence& sn, float* ring, T* orig,
-                                               const float* table, int lane) {
+__device__ __forceinline__ bool batch_dispatch(const TrainParams& p, const Sentence& sn, float* ring, T* orig,
+                                               const float* table, int lane, uint32_t bar, uint32_t& phase) {
   if constexpr (FAMILY == 0) {
-    if (p.lane_vec == 2) batch_stages<T, 2, 1>(p, sn, ring, orig, table, lane);
-    else batch_stages<T, 4, 1>(p, sn, ring, orig, table, lane);
+    if (p.lane_vec == 2) return batch_stages<T, 2, 1>(p, sn, ring, orig, table, lane, bar, phase);
+    return batch_stages<T, 4, 1>(p, sn, ring, orig, table, lane, bar, phase);
   } else if constexpr (FAMILY == 1) {
-    if (p.lane_nv == 3) {
-      train_sentence<T, 4, 3, 2, 0>(p, sn, ring, orig, table, lane);
-    } else {
-      if (p.stages == 2) train_sentence<T, 4, 2, 2, 0>(p, sn, ring, orig, table, lane);
-      else train_sentence<T, 4, 2, 3, 0>(p, sn, ring, orig, table, lane);
-    }
+    if (p.lane_nv == 3) return train_sentence<T, 4, 3, 2, 0>(p, sn, ring, orig, table, lane, bar, phase);
+    if (p.stages == 2) return train_sentence<T, 4, 2, 2, 0>(p, sn, ring, orig, table, lane, bar, phase);
+    return train_sentence<T, 4, 2, 3, 0>(p, sn, ring, orig, table, lane, bar, phase);
   } else {
     if (p.lane_nv == 3) {
-      if (p.stages == 3) train_sentence<T, 4, 3, 3, 0>(p, sn, ring, orig, table, lane);
-      else train_sentence<T, 4, 3, 4, 0>(p, sn, ring, orig, table, lane);
-    } else {
-      if (p.stages == 4) train_sentence<T, 4, 2, 4, 0>(p, sn, ring, orig, table, lane);
-      else train_sentence<T, 4, 2, 6, 0>(p, sn, ring, orig, table, lane);
+      if (p.stages == 3) return train_sentence<T, 4, 3, 3, 0>(p, sn, ring, orig, table, lane, bar, phase);
+      return train_sentence<T, 4, 3, 4, 0>(p, sn, ring, orig, table, lane, bar, phase);
     }
+    if (p.stages == 4) return train_sentence<T, 4, 2, 4, 0>(p, sn, ring, orig, table, lane, bar, phase);
+    return train_sentence<T, 4, 2, 6, 0>(p, sn, ring, orig, table, lane, bar, phase);
   }
 }
 
@@ -124,6 +121,9 @@ __global__ void __launch_bounds__(BatchFamily<FAMILY>::kMaxWarps * 32, BatchFami
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   if (a.deterministic && gwarp != 0) return;
   if (gwarp >= a.scratch_warps) return;
+  // the mbarrier at the end of the warp's region (every job's layout fits before it)
+  const uint32_t bar = warp_bulk_init(ring, (uint32_t)(a.smem_floats * 4), lane);
+  uint32_t phase = 0;
   int cur = -1;
   int64_t next = gwarp;
   for (;;) {
@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(BatchFamily<FAMILY>::kMaxWarps * 32, BatchFami
     sn.len = a.ent_len[slot];
     sn.alpha = a.ent_alpha[slot];
     sn.uid = a.uid_base[lo] + e;
-    batch_dispatch<T, FAMILY>(tp[warp], sn, ring, orig, a.exp_table, lane);
+    if (!batch_dispatch<T, FAMILY>(tp[warp], sn, ring, orig, a.exp_table, lane, bar, phase)) break;
   }
 }
 

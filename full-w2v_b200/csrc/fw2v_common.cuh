@@ -212,6 +212,7 @@ struct TrainParams {
   uint64_t sr_seed;  // stochastic rounding of bfloat16 write-backs
   int bf16;          // tables hold bfloat16
   int prefetch;      // copy each group's target rows while the previous group trains
+  int bulk;          // stage the entering and leaving context rows by bulk copies
   // batched launches: lane vector width (2 or 4), vectors per lane (1 to 3)
   // and pipeline stages of this job's sentences
   int lane_vec, lane_nv, stages;

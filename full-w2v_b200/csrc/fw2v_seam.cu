@@ -128,5 +128,5 @@ extern "C" fw2v_status fw2v_kernel_batch_error(void* stream) {
   if (cudaMemcpyFromSymbol(&flag, g_seam_error, sizeof(int)) != cudaSuccess) return FW2V_ERR_CUDA;
   if (!flag) return FW2V_OK;
   if (cudaMemcpyToSymbol(g_seam_error, &zero, sizeof(int)) != cudaSuccess) return FW2V_ERR_CUDA;
-  return FW2V_ERR_BOUNDS;
+  return flag == 2 ? FW2V_ERR_CUDA : FW2V_ERR_BOUNDS;  // 2: a bulk row copy did not complete in time
 }

@@ -165,6 +165,22 @@ struct LaneMap {
   }
 };
 
+// A row staged by a bulk copy holds the table row's padding past d; the one
+// lane whose vector straddles d (d not a multiple of VEC) clears it.
+template <int VEC, int NV>
+__device__ __forceinline__ void clear_past_d(Row<VEC, NV>& r, const LaneMap<VEC, NV>& m, int d) {
+  if ((d & (VEC - 1)) == 0) return;
+#pragma unroll
+  for (int i = 0; i < NV; i++) {
+    const int e = (int)(m.off[i] / 4);
+    if (e < d && e + VEC > d) {
+#pragma unroll
+      for (int j = 0; j < VEC; j++)
+        if (e + j >= d) r.x[i][j] = 0.0f;
+    }
+  }
+}
+
 // Rows of one vector per lane (d <= 128) test the lane with a branch, which
 // is the same on every lane when d fills the warp.  The last vector of wider
 // rows, which ends inside the row on some lanes only, is loaded from the zero
@@ -261,6 +277,51 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 // All but the most recently committed group complete.
 __device__ __forceinline__ void cp_async_wait_but_last() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Bulk copies (cp.async.bulk, the async proxy; non-multicast, this GPU's own
+// memory only) of whole staged rows, issued by one lane.  Loads complete on
+// a per-warp mbarrier (transaction bytes); stores are bulk groups.
+__device__ __forceinline__ void mbar_init(uint32_t bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for phase `parity` of the barrier, at most kBulkWaitTries tries
+// (each try suspends the thread for a bounded time): false if it gave up.
+constexpr int kBulkWaitTries = 1 << 22;
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (int i = 0; i < kBulkWaitTries; i++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_store(void* dst, uint32_t src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// The bulk stores' reads of shared memory are done / all but the latest
+// group's stores are complete / all are complete.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_but_last() { asm volatile("cp.async.bulk.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// Orders this thread's generic-proxy accesses (shared and global) with
+// async-proxy accesses on either side of it.
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async;" ::: "memory"); }
 
 template <int VEC, int NV>
 __device__ __forceinline__ void row_zero(Row<VEC, NV>& r) {
@@ -784,9 +845,22 @@ __device__ __forceinline__ void sts_staged(const Row<VEC, NV>& r, uint32_t row, 
 // Shared memory of one warp, rows of `pitch` elements: the FP32 ring of
 // D = 2W+1 rows and a sink row, then staged rows of the table's element type
 // (R target originals, 2 x R with the target prefetch, and 2 staging rows),
-// then a 16-byte zero vector.
+// then a 16-byte zero vector and the 16-byte slot of the warp's mbarrier.
 __host__ __device__ constexpr int64_t warp_smem_bytes(int D, int R, bool prefetch, int64_t pitch, int elem) {
-  return (int64_t)(D + 1) * pitch * 4 + (int64_t)((prefetch ? 2 : 1) * R + 2) * pitch * elem + 16;
+  return (int64_t)(D + 1) * pitch * 4 + (int64_t)((prefetch ? 2 : 1) * R + 2) * pitch * elem + 32;
+}
+
+// The warp's mbarrier in the last 16 bytes of its shared-memory region of
+// region_bytes, initialised once per kernel (an mbarrier is not
+// re-initialised while the warp uses it): returns its address.
+__device__ __forceinline__ uint32_t warp_bulk_init(const float* region, uint32_t region_bytes, int lane) {
+  const uint32_t bar = smem_addr(region) + region_bytes - 16u;
+  if (lane == 0) {
+    mbar_init(bar);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncwarp();
+  return bar;
 }
 
 // One sentence on one warp.
@@ -794,14 +868,18 @@ __host__ __device__ constexpr int64_t warp_smem_bytes(int D, int R, bool prefetc
 //            value of sentence position p while it is in the window; slot D
 //            is a sink that the pipeline reads and writes on its idle steps;
 //            then the R target rows as loaded (for their write-back), two
-//            staging rows filled by cp.async (the entering row and the leaving
-//            row's original value) and the zero vector that lanes read in
+//            staging rows filled by bulk copies (the entering row and the
+//            leaving row's original value), the zero vector that lanes read in
 //            place of vectors past d.
 //   orig     this warp's global scratch, D rows: the value each slot's row had
 //            when it entered the window (needed for its single write-back).
+// Returns false if a bulk copy did not complete in time (the error word is
+// set to 2): the warp then stops.
+//   bar_b    the warp's mbarrier (initialised once per kernel by warp_bulk_init)
+//            and bar_phase its phase parity, carried from sentence to sentence.
 template <typename T, int VEC, int NV, int R, int SIG>
-__device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* ring, T* orig,
-                               const float* table, int lane) {
+__device__ bool train_sentence(const TrainParams& p, const Sentence& sn, float* ring, T* orig,
+                               const float* table, int lane, uint32_t bar_b, uint32_t& bar_phase) {
   constexpr int RP = PadPow2<R>::value;
   const int W = p.window, K = p.negative, D = 2 * W + 1;
   const int P = (int)p.pitch;  // row stride, global and shared
@@ -814,6 +892,8 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   const float alpha = sn.alpha;
   const bool one_group = K + 1 <= R;
   const bool pre = p.prefetch != 0;  // target rows copied one group of targets ahead
+  // context rows staged by bulk copies (lane 0, mbarrier) instead of per-lane cp.async
+  const bool bulk = p.bulk != 0;
   const uint64_t skey = sr_sentence_key(p.sr_seed, (uint64_t)sn.uid);  // bfloat16 tables only
 
   // Every id is checked before any table access.
@@ -828,9 +908,9 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   }
   if (__any_sync(kFull, bad)) {
     if (lane == 0) atomicExch(p.error_flag, 1);
-    return;
+    return true;
   }
-  if (L <= 0) return;
+  if (L <= 0) return true;
 
   Row<VEC, NV> tmp;
   const int n_enter = W + 1 < L ? W + 1 : L;
@@ -856,6 +936,10 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
   const uint32_t in_b = pre ? o1_b + (uint32_t)R * srow_bytes : o1_b;
   const uint32_t out_b = in_b + srow_bytes;
   const uint32_t zero_b = out_b + srow_bytes;
+  // The entering row and the leaving row's original arrive by bulk copies
+  // (lane 0) that complete on the warp's mbarrier, one phase per centre that
+  // has any; the entering row goes on to the originals scratch by a bulk store.
+  int last_store_slot = -1;  // the slot whose original the latest bulk store wrote
   if (lane < 4) asm volatile("st.shared.f32 [%0], %1;" ::"r"(zero_b + 4u * lane), "f"(0.0f) : "memory");
   __syncwarp();
   const LaneMap<VEC, NV> lm(lane, d, zero_b);
@@ -904,9 +988,29 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
     // the same word (its write-back must land first).  Both staging copies run
     // in the background while the centre trains.
     const bool enter_early = id_in >= 0 && id_in != id_out;
-    if (enter_early) cp_row(in_b, syn0 + (int64_t)id_in * P, lm, d);
-    if (q_out >= 0) cp_row(out_b, orig + slot_out * P, lm, d);
-    cp_async_commit();
+    const uint32_t stage_bytes = bulk ? (enter_early ? srow_bytes : 0u) + (q_out >= 0 ? srow_bytes : 0u) : 0u;
+    if (!bulk) {
+      if (enter_early) cp_row(in_b, syn0 + (int64_t)id_in * P, lm, d);
+      if (q_out >= 0) cp_row(out_b, orig + slot_out * P, lm, d);
+      cp_async_commit();
+    } else if (stage_bytes) {
+      // every lane's generic accesses so far (its reads of the staging rows,
+      // its stores and write-backs to the tables and the originals scratch)
+      // before the async-proxy copies
+      proxy_fence();
+      __syncwarp();
+      if (lane == 0) {
+        // the last bulk store has read the entering row's staging row, and
+        // the leaving row's original is written: every store but the latest
+        // is complete, and the latest too if it was this slot's
+        if (q_out >= 0 && slot_out == last_store_slot) bulk_wait_all();
+        else bulk_wait_but_last();
+        bulk_wait_read();
+        mbar_expect_tx(bar_b, stage_bytes);
+        if (enter_early) bulk_load(in_b, syn0 + (int64_t)id_in * P, srow_bytes, bar_b);
+        if (q_out >= 0) bulk_load(out_b, orig + slot_out * P, srow_bytes, bar_b);
+      }
+    }
 
     // Lane r < D decides whether ring slot r holds a context of centre w.
     const int base = w - W;
@@ -925,8 +1029,8 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
         const int my_t = one_group ? t_here : target_id(ids, negs, K, w, k0, nt, lane);
         if (pre) {
           // This group's rows: committed before this centre's staging copies
-          // for its first group, before the previous group's prefetch otherwise.
-          if (k0 == 0) cp_async_wait_but_last();
+          // (per-lane staging) for its first group, else the latest group.
+          if (k0 == 0 && !bulk) cp_async_wait_but_last();
           else cp_async_wait();
           // A row copied before the previous group's write-back of the same
           // target is fetched again (after this lane's own reduction, in
@@ -1065,27 +1169,54 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
 
     // Slide the window: position w-W leaves, position w+W+1 takes its slot.
     // The staging copies must be complete; the next group's prefetch may run on.
-    if (prefetches > 0) cp_async_wait_but_last();
-    else cp_async_wait();
+    if (!bulk) {
+      if (prefetches > 0) cp_async_wait_but_last();
+      else cp_async_wait();
+    } else if (stage_bytes) {
+      if (!mbar_wait(bar_b, bar_phase)) {
+        // give the copies a second bounded wait before the warp stops
+        if (lane == 0) atomicExch(p.error_flag, 2);
+        mbar_wait(bar_b, bar_phase);
+        if (lane == 0) bulk_wait_all();
+        __syncwarp();
+        return false;
+      }
+      bar_phase ^= 1u;
+    }
     if (q_out >= 0) {
       Row<VEC, NV> cur, org;
       lds_row(cur, ring_b + (uint32_t)slot_out * row_bytes, lm);
       lds_staged<T>(org, out_b, lm);
+      if (bulk) clear_past_d(org, lm, d);
       row_add_delta(syn0 + (int64_t)id_out * P, cur, org, lane, d,
                     sr_event_key(skey, (uint64_t)L * (K + 1) + q_out), (uint64_t)id_out);
     }
     if (id_in >= 0) {
       const int s = slot_out;
       Row<VEC, NV> enter_row;
-      if (enter_early) lds_staged<T>(enter_row, in_b, lm);
-      else row_load_global(enter_row, syn0 + (int64_t)id_in * P, lane, d);
+      if (enter_early) {
+        lds_staged<T>(enter_row, in_b, lm);
+        if (bulk) {
+          clear_past_d(enter_row, lm, d);
+          if (lane == 0) bulk_store(orig + s * P, in_b, srow_bytes);
+          last_store_slot = s;
+        } else {
+          row_store_global(enter_row, orig + s * P, lane, d);
+        }
+      } else {
+        row_load_global(enter_row, syn0 + (int64_t)id_in * P, lane, d);
+        row_store_global(enter_row, orig + s * P, lane, d);
+      }
       sts_row(enter_row, ring_b + (uint32_t)s * row_bytes, lm);
-      row_store_global(enter_row, orig + s * P, lane, d);
     }
     slot_out = slot_out + 1 < D ? slot_out + 1 : 0;
     lane_off = lane_off > 0 ? lane_off - 1 : D - 1;
   }
-  // Positions still in the window leave in increasing order.
+  // Positions still in the window leave in increasing order; their originals
+  // are read back with generic loads once the bulk stores are complete.
+  if (lane == 0) bulk_wait_all();
+  __syncwarp();
+  proxy_fence();
   for (int q = L - W > 0 ? L - W : 0; q < L; q++) {
     const int s = q % D;
     Row<VEC, NV> cur, org;
@@ -1095,6 +1226,7 @@ __device__ void train_sentence(const TrainParams& p, const Sentence& sn, float* 
     row_add_delta(syn0 + (int64_t)id_q * P, cur, org, lane, d,
                   sr_event_key(skey, (uint64_t)L * (K + 1) + q), (uint64_t)id_q);
   }
+  return true;
 }
 
 // Blocks per SM the register budget is sized for: the one-vector shapes fit
@@ -1124,6 +1256,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MinBlocks<NV>::value) sgn
   const int64_t total = total_sentences(p);
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   if (p.deterministic && gwarp != 0) return;
+  const uint32_t bar_b =
+      warp_bulk_init(ring, (uint32_t)warp_smem_bytes(D, R, p.prefetch != 0, p.pitch, (int)sizeof(T)), lane);
+  uint32_t bar_phase = 0;
   int64_t next = gwarp;
   for (;;) {
     int64_t w;
@@ -1139,7 +1274,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MinBlocks<NV>::value) sgn
     }
     if (w >= total) break;
     const Sentence sn = fetch_sentence(p, w);
-    train_sentence<T, VEC, NV, R, SIG>(sp, sn, ring, orig, p.exp_table, lane);
+    if (!train_sentence<T, VEC, NV, R, SIG>(sp, sn, ring, orig, p.exp_table, lane, bar_b, bar_phase)) break;
   }
 }
 

@@ -349,10 +349,12 @@ fw2v_status fw2v_batch_add_job_device(fw2v_batch* b, const fw2v_config* cfg, con
 /* A job's kernel shape: the lane vector width and vectors per lane (2 x 1:
  * 32 lanes of 2 floats cover d <= 64; 4 x 1: d <= 128, 16 lanes suffice for
  * d <= 64; 4 x 2: d <= 256; 4 x 3: d <= 384), the pipeline stages (2, 3, 4
- * or 6 targets in flight; 4 at most with 3 vectors per lane) and the target
- * prefetch (1: the target rows of each group of `stages` targets are copied
- * into shared memory while the previous group trains).  Defaults follow d and
- * negative, prefetch off;
+ * or 6 targets in flight; 4 at most with 3 vectors per lane) and the staging
+ * bits `prefetch`: bit 0, the target rows of each group of `stages` targets
+ * are copied into shared memory while the previous group trains; bit 1, the
+ * entering context row and the leaving row's original are staged by
+ * cp.async.bulk copies from one lane (completion on an mbarrier) instead of
+ * per-lane cp.async.  Defaults follow d and negative, both bits off;
  * fw2v_batch_tune picks them by measurement. */
 fw2v_status fw2v_batch_set_shape(fw2v_batch* b, int32_t job, int32_t lane_vec, int32_t lane_nv, int32_t stages,
                                  int32_t prefetch);

@@ -132,7 +132,10 @@ def test_deterministic_batch_equals_each_job_alone_bf16(jobs, group_bytes):
 SHAPES = ([(2, (2, 1, s, 0)) for s in (2, 3, 4, 6)] + [(2, (4, 1, s, 0)) for s in (2, 3, 4, 6)] +
           [(5, (4, 2, s, 0)) for s in (2, 3, 4, 6)] + [(6, (4, 3, s, 0)) for s in (2, 3, 4)] +
           [(2, (2, 1, 6, 1)), (2, (4, 1, 6, 1)), (5, (4, 2, 6, 1)), (3, (4, 1, 6, 1)),
-           (2, (2, 1, 2, 1)), (2, (4, 1, 3, 1)), (5, (4, 2, 3, 1)), (6, (4, 3, 2, 1)), (6, (4, 3, 4, 1))])
+           (2, (2, 1, 2, 1)), (2, (4, 1, 3, 1)), (5, (4, 2, 3, 1)), (6, (4, 3, 2, 1)), (6, (4, 3, 4, 1))] +
+          # bit 1: context rows staged by bulk copies (short sentences of job 5, walks of jobs 3 and 6)
+          [(5, (4, 2, 3, 2)), (5, (4, 2, 6, 3)), (6, (4, 3, 2, 3)), (2, (2, 1, 6, 2)), (3, (4, 1, 6, 3)),
+           (1, (2, 1, 4, 3))])
 
 
 @pytest.mark.parametrize("job,shape", SHAPES)
