@@ -313,7 +313,7 @@ def run_own(args, world, rank, local):
                 b.set_shape(0, *[int(x) for x in args.shape.split(",")])
                 if args.wpb:
                     for f in range(3):
-                        b.set_launch(f, min(args.wpb, 8 if f == 0 else 4))
+                        b.set_launch(f, min(args.wpb, (8, 6, 4)[f]))
                 tuned = {"given": args.shape, "warps_per_block": args.wpb}
             else:
                 tuned = b.tune(cache=tune_cache)
@@ -371,7 +371,7 @@ def run_own(args, world, rank, local):
                     eb.set_shape(0, *[int(x) for x in args.shape.split(",")])
                     if args.wpb:
                         for f in range(3):
-                            eb.set_launch(f, min(args.wpb, 8 if f == 0 else 4))
+                            eb.set_launch(f, min(args.wpb, (8, 6, 4)[f]))
                 else:
                     eb.tune(cache=tune_cache)  # the shapes chosen above, from the cache
                 st = eb.train_epochs(1)

@@ -182,7 +182,8 @@ struct fw2v_batch {
   int64_t buf_kept_cap = 0, buf_stream_cap = 0;
   void* orig_scratch = nullptr;
   int64_t scratch_elems = 0, scratch_warps = 0, scratch_bytes = 0;
-  int warps_per_block[kBatchFamilies] = {4, 4, 4}, blocks_per_sm[kBatchFamilies] = {0, 0, 0};  // per family
+  // per family; 0 warps: the count that keeps the most warps resident
+  int warps_per_block[kBatchFamilies] = {0, 0, 0}, blocks_per_sm[kBatchFamilies] = {0, 0, 0};
   int epochs_run = 0;  // batch epochs trained so far: job j has trained min(epochs_run, its epochs)
   int next_buf = 0;  // the buffer set of the next round
   std::vector<unsigned long long> words_snap, kept_snap;  // counters at the end of the last call
@@ -471,16 +472,39 @@ fw2v_status grid_for(fw2v_batch* b, const std::vector<int>& active, int fam, int
   if (g->smem_floats == 0) return FW2V_OK;
   const int det = b->cfg.deterministic;
   cudaError_t e = cudaErrorInvalidValue;
-#define FW2V_GRID(T, F)                                                                                  \
-  if (fam == F)                                                                                         \
-    e = batch_grid<T, F>(g->smem_floats, wpb, cap, b->num_sms, b->scratch_warps, det, &g->blocks, &g->threads, \
-                         &g->smem);
-  if (b->elem == 2) {
-    FW2V_GRID(bf16_t, 0) FW2V_GRID(bf16_t, 1) FW2V_GRID(bf16_t, 2)
-  } else {
-    FW2V_GRID(float, 0) FW2V_GRID(float, 1) FW2V_GRID(float, 2)
-  }
+  auto grid = [&](int w, Grid* out) {
+    cudaError_t r = cudaErrorInvalidValue;
+#define FW2V_GRID(T, F)                                                                                      \
+  if (fam == F)                                                                                             \
+    r = batch_grid<T, F>(out->smem_floats, w, cap, b->num_sms, b->scratch_warps, det, &out->blocks, &out->threads, \
+                         &out->smem);
+    if (b->elem == 2) {
+      FW2V_GRID(bf16_t, 0) FW2V_GRID(bf16_t, 1) FW2V_GRID(bf16_t, 2)
+    } else {
+      FW2V_GRID(float, 0) FW2V_GRID(float, 1) FW2V_GRID(float, 2)
+    }
 #undef FW2V_GRID
+    return r;
+  };
+  if (wpb > 0) {
+    e = grid(wpb, g);
+  } else {
+    // automatic: the most resident warps (blocks x warps), the larger block on
+    // a tie; every try sets the kernel's shared-memory limit, so the chosen
+    // count is set up again last
+    int64_t most = 0;
+    int best = 0;
+    for (int w : {8, 6, 4, 2}) {
+      if (w > batch_max_warps(fam)) continue;
+      Grid t = *g;
+      if (grid(w, &t) != cudaSuccess) continue;
+      if ((int64_t)t.blocks * (t.threads / 32) > most) {
+        most = (int64_t)t.blocks * (t.threads / 32);
+        best = w;
+      }
+    }
+    if (best > 0) e = grid(best, g);
+  }
   if (e != cudaSuccess)
     return bfail(b, FW2V_ERR_ARGUMENT, "batch grid (%d warps per block, %lld floats per warp): %s", wpb,
                  (long long)g->smem_floats, cudaGetErrorString(e));
@@ -855,10 +879,10 @@ fw2v_status fw2v_batch_get_shape(fw2v_batch* b, int32_t job, int32_t* lane_vec, 
 }
 
 fw2v_status fw2v_batch_set_launch(fw2v_batch* b, int32_t family, int32_t warps_per_block, int32_t blocks_per_sm) {
-  const int max_w = family == 0 ? BatchFamily<0>::kMaxWarps : BatchFamily<1>::kMaxWarps;
-  if (!b || family < 0 || family >= kBatchFamilies || warps_per_block < 1 || warps_per_block > max_w ||
-      blocks_per_sm < 0)
-    return bfail(b, FW2V_ERR_ARGUMENT, "family 0..2, warps per block 1..8 (1..4 for wide rows), blocks per SM >= 0");
+  if (!b || family < 0 || family >= kBatchFamilies || warps_per_block < 0 ||
+      warps_per_block > batch_max_warps(family) || blocks_per_sm < 0)
+    return bfail(b, FW2V_ERR_ARGUMENT,
+                 "family 0..2, warps per block 0 (automatic) or 1..8, 1..6, 1..4 (families 0, 1, 2), blocks per SM >= 0");
   b->warps_per_block[family] = warps_per_block;
   b->blocks_per_sm[family] = blocks_per_sm;
   return FW2V_OK;
@@ -908,6 +932,10 @@ fw2v_status fw2v_batch_train_epochs(fw2v_batch* b, int32_t n_epochs, fw2v_batch_
     BCK(b, cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
     const cudaError_t e = enqueue_epochs(b, e0, epochs, g, true);
     const cudaError_t e2 = cudaStreamEndCapture(b->st, &graph);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();  // the failed capture's error is reported here, not by a later call
+    }
     BCK(b, e);
     BCK(b, e2);
     cudaError_t e3 = cudaGraphInstantiate(&exec, graph, 0);
@@ -1186,9 +1214,9 @@ extern "C" fw2v_status fw2v_batch_tune(fw2v_batch* b, int64_t sample_tokens, fw2
     if (result == FW2V_OK) result = sample_into_buf0(r);
     double best = -1;
     int best_w = b->warps_per_block[fam];
-    for (int w : {2, 4, 8}) {
+    for (int w : {2, 4, 6, 8}) {
       if (result != FW2V_OK) break;
-      if (fam != 0 && w > BatchFamily<1>::kMaxWarps) continue;
+      if (w > batch_max_warps(fam)) continue;
       Grid g;
       if (grid_for(b, act, fam, w, 0, &g) != FW2V_OK) continue;  // does not fit: skip
       float ms = 0;

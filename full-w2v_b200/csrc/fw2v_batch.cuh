@@ -46,7 +46,8 @@ constexpr int kBatchStages[] = {2, 3, 4, 6};
 //   0  rows of one vector per lane (d <= 128: 2-float lanes for d <= 64,
 //      4-float for d <= 128), up to 8 warps per block, 128 registers
 //   1  wide rows: 2 four-float vectors per lane with 2 or 3 stages, 3 vectors
-//      with 2; 4 warps per block, 3 blocks per SM
+//      with 2; up to 6 warps per block, 168 registers (12 warps per SM: 2
+//      blocks of 6, or 3 of 4)
 //   2  other wide rows (2 vectors: 4 or 6 stages; 3 vectors: 3 or 4); 4 warps
 //      per block, 255 registers
 constexpr int kBatchMaxWarps = 8;
@@ -59,12 +60,16 @@ struct BatchFamily<0> {
 };
 template <>
 struct BatchFamily<1> {
-  static constexpr int kMaxWarps = 4, kMinBlocks = 3;
+  static constexpr int kMaxWarps = 6, kMinBlocks = 2;
 };
 template <>
 struct BatchFamily<2> {
   static constexpr int kMaxWarps = 4, kMinBlocks = 2;
 };
+
+__host__ __device__ constexpr int batch_max_warps(int family) {
+  return family == 0 ? BatchFamily<0>::kMaxWarps : family == 1 ? BatchFamily<1>::kMaxWarps : BatchFamily<2>::kMaxWarps;
+}
 
 // The family of a (lane vector width, vectors per lane, stages) shape.
 __host__ __device__ constexpr int batch_family(int nv, int stages) {
@@ -112,6 +117,9 @@ __global__ void __launch_bounds__(BatchFamily<FAMILY>::kMaxWarps * 32, BatchFami
     sgns_batch_kernel(BatchTrainArgs a) {
   extern __shared__ __align__(16) float smem[];
   __shared__ __align__(8) TrainParams tp[BatchFamily<FAMILY>::kMaxWarps];
+  __shared__ float table[kExpTableSize];  // the sigmoid table, read once per pipeline step
+  for (int i = threadIdx.x; i < kExpTableSize; i += blockDim.x) table[i] = a.exp_table[i];
+  __syncthreads();
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   float* ring = smem + (int64_t)warp * a.smem_floats;
@@ -161,7 +169,7 @@ __global__ void __launch_bounds__(BatchFamily<FAMILY>::kMaxWarps * 32, BatchFami
     sn.len = a.ent_len[slot];
     sn.alpha = a.ent_alpha[slot];
     sn.uid = a.uid_base[lo] + e;
-    if (!batch_dispatch<T, FAMILY>(tp[warp], sn, ring, orig, a.exp_table, lane, bar, phase)) break;
+    if (!batch_dispatch<T, FAMILY>(tp[warp], sn, ring, orig, table, lane, bar, phase)) break;
   }
 }
 
@@ -177,7 +185,16 @@ cudaError_t batch_grid(int64_t smem_floats, int warps, int per_sm_cap, int num_s
   if (warps < 1 || warps > BatchFamily<FAMILY>::kMaxWarps) return cudaErrorInvalidValue;
   *smem = (size_t)warps * (size_t)smem_floats * sizeof(float);
   *threads = warps * 32;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+  // A block that does not fit is refused here, before any CUDA call can fail
+  // and leave its error to be read back after a later launch.
+  int dev = 0, optin = 0;
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kern);
+  if (e != cudaSuccess) return e;
+  if (*smem + fa.sharedSizeBytes > (size_t)optin) return cudaErrorInvalidValue;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
   if (e != cudaSuccess) return e;
   if (deterministic) {
     *blocks = 1;

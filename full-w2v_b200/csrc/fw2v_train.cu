@@ -86,7 +86,7 @@ size_t launch_warp_smem(const TrainParams& p) {
 // Whether one warp of a launch of p fits a block's shared memory (launch_t
 // takes 4, 2 or 1 warps per block, as many as fit).
 bool launch_fits(const TrainParams& p) {
-  return train_block_warps(launch_warp_smem(p), sizeof(TrainParams) + 64, 1) == 1;
+  return train_block_warps(launch_warp_smem(p), sizeof(TrainParams) + kExpTableSize * sizeof(float) + 64, 1) == 1;
 }
 
 cudaError_t launch_train(const TrainParams& p, int num_sms, cudaStream_t st) {

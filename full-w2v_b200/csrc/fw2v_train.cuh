@@ -580,16 +580,46 @@ __device__ __forceinline__ void row_update(Row<VEC, NV>& v, Row<VEC, NV>& o, flo
 
 // alpha * (label - sigma(x)).  Table mode reproduces FULL-W2V-kernels.cu:92-99:
 // index = (int)(saturate((x + 6) / 12) * 999); the positive target reads the
-// reversed table (nexpTable[i] == expTable[999 - i]).
+// reversed table (nexpTable[i] == expTable[999 - i]).  `table` is the block's
+// shared-memory copy.
 template <int SIG>
 __device__ __forceinline__ float gradient(float x, bool positive, float alpha, const float* table) {
   if constexpr (SIG == 0) {
     const float s = __saturatef(__fmul_rn(__fadd_rn(x, 6.0f), 1.0f / 12.0f));
     const int idx = __float2int_rz(__fmul_rn(s, 999.0f));
-    return positive ? __fmul_rn(alpha, __ldg(table + (kExpTableSize - 1 - idx))) : __fmul_rn(-alpha, __ldg(table + idx));
+    return positive ? __fmul_rn(alpha, table[kExpTableSize - 1 - idx]) : __fmul_rn(-alpha, table[idx]);
   }
   return positive ? __fdiv_rn(alpha, __fadd_rn(1.0f, expf(x)))
                   : __fdiv_rn(-alpha, __fadd_rn(1.0f, expf(-x)));
+}
+
+// The table-mode gradient of a pipeline stage with its constant parts folded
+// in ahead of the step, so that the dependent chain from the dot product to g
+// is FADD, FMUL (saturating), FMUL, FADD, IMAD, shared-memory load, FMUL:
+//   * the truncation (int)y of y = s * 999 in [0, 999] is read from the bits
+//     of y + 2^23 added toward zero: 0x4B000000 + (int)y;
+//   * the entry address is a + b * bits (32-bit wrap-around), with b = 4 and
+//     a = table - 4 * 0x4B000000 for a negative target, b = -4 and
+//     a = table + 4 * 999 + 4 * 0x4B000000 for the positive one (which reads
+//     the table reversed);
+//   * alpha_k is alpha (positive), -alpha (negative) or 0 (an idle stage:
+//     g = +0 exactly as a skipped step).
+// The result is bit-identical to gradient<0>.
+struct TableStage {
+  uint32_t a, b;
+};
+__device__ __forceinline__ TableStage table_stage(uint32_t table_b, bool positive) {
+  TableStage t;
+  t.b = positive ? (uint32_t)-4 : 4u;
+  t.a = positive ? table_b + 4u * (uint32_t)(kExpTableSize - 1) + 4u * 0x4B000000u : table_b - 4u * 0x4B000000u;
+  return t;
+}
+__device__ __forceinline__ float table_gradient(float x, const TableStage& t, float alpha_k) {
+  const float s = __saturatef(__fmul_rn(__fadd_rn(x, 6.0f), 1.0f / 12.0f));
+  const float y = __fadd_rz(__fmul_rn(s, 999.0f), 8388608.0f);
+  float e;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(e) : "r"(t.a + t.b * __float_as_uint(y)));
+  return __fmul_rn(alpha_k, e);
 }
 
 struct Sentence {
@@ -920,6 +950,7 @@ __device__ bool train_sentence(const TrainParams& p, const Sentence& sn, float* 
     row_store_global(tmp, orig + q * P, lane, d);
   }
   const uint32_t ring_b = smem_addr(ring);
+  const uint32_t table_b = smem_addr(table);  // the block's shared copy of the sigmoid table
   const uint32_t row_bytes = (uint32_t)P * 4u;
   // staged rows (target originals, entering and leaving copies) hold the
   // table's element type: half size with bfloat16 tables
@@ -1087,6 +1118,8 @@ __device__ bool train_sentence(const TrainParams& p, const Sentence& sn, float* 
           }
           const int my_stage = stage_of_lane<RP>(lane);
           const bool my_positive = k0 + my_stage == 0;
+          const TableStage my_tab = table_stage(table_b, my_positive);
+          const float my_alpha = my_positive ? alpha : -alpha;
           // the lane's stage is active at steps [my_stage, my_stage + nctx)
           const unsigned my_span = my_stage < nt ? (unsigned)nctx : 0u;
           unsigned rem = mask;
@@ -1110,7 +1143,9 @@ __device__ bool train_sentence(const TrainParams& p, const Sentence& sn, float* 
                 });
                 const float xs = transpose_reduce<RP>(x, lane);
                 const bool act = (unsigned)(ts - my_stage) < my_span;
-                const float g = act ? gradient<SIG>(xs, my_positive, alpha, table) : 0.0f;
+                float g;
+                if constexpr (SIG == 0) g = table_gradient(xs, my_tab, act ? my_alpha : 0.0f);
+                else g = act ? gradient<SIG>(xs, my_positive, alpha, table) : 0.0f;
                 // every lane needs every stage's g; with two stages the other
                 // half-warp holds the other one
                 float g_other = 0.0f;
@@ -1245,7 +1280,10 @@ template <typename T, int VEC, int NV, int R, int SIG>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, MinBlocks<NV>::value) sgns_train_kernel(TrainParams p) {
   extern __shared__ __align__(16) float smem[];
   __shared__ __align__(8) TrainParams sp;
+  __shared__ float table[kExpTableSize];  // the sigmoid table, read once per pipeline step
   copy_params(&sp, &p, threadIdx.x, blockDim.x);
+  if constexpr (SIG == 0)
+    for (int i = threadIdx.x; i < kExpTableSize; i += blockDim.x) table[i] = p.exp_table[i];
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -1274,7 +1312,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MinBlocks<NV>::value) sgn
     }
     if (w >= total) break;
     const Sentence sn = fetch_sentence(p, w);
-    if (!train_sentence<T, VEC, NV, R, SIG>(sp, sn, ring, orig, p.exp_table, lane, bar_b, bar_phase)) break;
+    if (!train_sentence<T, VEC, NV, R, SIG>(sp, sn, ring, orig, table, lane, bar_b, bar_phase)) break;
   }
 }
 

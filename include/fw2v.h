@@ -363,8 +363,10 @@ fw2v_status fw2v_batch_get_shape(fw2v_batch* b, int32_t job, int32_t* lane_vec, 
 
 /* The training grid of a kernel family (0: one vector per lane; 1: wide rows
  * with 2 or 3 stages (2 vectors per lane) or 2 stages (3 vectors); 2: other
- * wide rows): warps per block (sentences trained side by side in one block,
- * 1..8, 1..4 for wide rows) and a cap on blocks per SM (0: as many as fit). */
+ * wide rows): warps per block (sentences trained side by side in one block:
+ * 1..8 in family 0, 1..6 in family 1, 1..4 in family 2; 0, the default: the
+ * count of 8, 6, 4 or 2 that keeps the most warps resident per SM) and a cap
+ * on blocks per SM (0: as many as fit). */
 fw2v_status fw2v_batch_set_launch(fw2v_batch* b, int32_t family, int32_t warps_per_block, int32_t blocks_per_sm);
 fw2v_status fw2v_batch_get_launch(fw2v_batch* b, int32_t family, int32_t* warps_per_block,
                                   int32_t* blocks_per_sm);
