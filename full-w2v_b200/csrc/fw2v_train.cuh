@@ -243,14 +243,15 @@ __device__ __forceinline__ void cp_row(uint32_t dst, const float* src, const Lan
   for (int i = 0; i < NV; i++) {
     const int e0 = (int)(m.off[i] / 4);
     if (vec_predicated<VEC, NV>(i, e0, d)) {
-      // whole, or a zero-byte copy (zero fill) into the zero vector
-      const bool on = e0 < d;
-      const uint32_t da = on ? dst + m.off[i] : m.zero;
-      const float* g = on ? src + e0 : src;
+      // whole, or nothing on lanes past d (their loads read the zero vector)
+      const uint32_t da = dst + m.off[i];
+      const float* g = src + e0;
       if constexpr (VEC == 4)
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(da), "l"(g), "r"(on ? 16 : 0) : "memory");
+        asm volatile("{ .reg .pred p; setp.ne.b32 p, %2, 0; @p cp.async.cg.shared.global [%0], [%1], 16; }"
+                     ::"r"(da), "l"(g), "r"((int)(e0 < d)) : "memory");
       else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(da), "l"(g), "r"(on ? 8 : 0) : "memory");
+        asm volatile("{ .reg .pred p; setp.ne.b32 p, %2, 0; @p cp.async.ca.shared.global [%0], [%1], 8; }"
+                     ::"r"(da), "l"(g), "r"((int)(e0 < d)) : "memory");
     } else if (m.ok[i]) {
       const float* g = src + m.off[i] / 4;
       if (vec_whole<VEC, NV>(i, (int)(m.off[i] / 4), d)) {
@@ -792,14 +793,15 @@ __device__ __forceinline__ void cp_row(uint32_t dst, const bf16_t* src, const La
   for (int i = 0; i < NV; i++) {
     const int e0 = (int)(m.off[i] / 4);
     if (vec_predicated<VEC, NV>(i, e0, d)) {
-      // whole, or a zero-byte copy (zero fill) into the zero vector
-      const bool on = e0 < d;
-      const uint32_t da = on ? dst + (uint32_t)e0 * 2u : m.zero;
-      const uint16_t* g = on ? h + e0 : h;
+      // whole, or nothing on lanes past d (their loads read the zero vector)
+      const uint32_t da = dst + (uint32_t)e0 * 2u;
+      const uint16_t* g = h + e0;
       if constexpr (VEC == 4)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(da), "l"(g), "r"(on ? 8 : 0) : "memory");
+        asm volatile("{ .reg .pred p; setp.ne.b32 p, %2, 0; @p cp.async.ca.shared.global [%0], [%1], 8; }"
+                     ::"r"(da), "l"(g), "r"((int)(e0 < d)) : "memory");
       else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(da), "l"(g), "r"(on ? 4 : 0) : "memory");
+        asm volatile("{ .reg .pred p; setp.ne.b32 p, %2, 0; @p cp.async.ca.shared.global [%0], [%1], 4; }"
+                     ::"r"(da), "l"(g), "r"((int)(e0 < d)) : "memory");
       continue;
     }
     if (!m.ok[i]) continue;
