@@ -24,6 +24,7 @@ cudaError_t launch_init_tables(void* syn0, bool bf16, int64_t V, int d, int64_t 
                                int n_firsts, int32_t* unigram, int64_t table_size, uint64_t start,
                                cudaStream_t st);
 size_t train_smem_bytes(int window, int64_t pitch, int warps, int r, bool prefetch, int elem);
+size_t train_static_smem();
 int64_t train_scratch_warps(int num_sms);
 cudaError_t launch_validate_ids(const int32_t* ids, int64_t n, int64_t vocab, int* flag, cudaStream_t st);
 cudaError_t launch_check_corpus(const int32_t* stream, int64_t len, const int64_t* chunk_off, int64_t n, int* flag,
@@ -247,7 +248,8 @@ fw2v_status fw2v_create(const fw2v_config* cfg, fw2v_handle** out) {
   if (cudaGetDeviceProperties(&prop, c.device) != cudaSuccess || prop.major != 10) return FW2V_ERR_NO_DEVICE;
   if (cudaSetDevice(c.device) != cudaSuccess) return FW2V_ERR_NO_DEVICE;
   const int64_t P = pitch_for(c.layer_size);
-  if (train_smem_bytes(c.window, P, 1, 8, false, 4) > (size_t)prop.sharedMemPerBlockOptin) return FW2V_ERR_ARGUMENT;
+  if (train_smem_bytes(c.window, P, 1, 8, false, 4) + train_static_smem() > (size_t)prop.sharedMemPerBlockOptin)
+    return FW2V_ERR_ARGUMENT;
   fw2v_handle* h = new fw2v_handle();
   h->cfg = c;
   h->elem = c.precision == FW2V_BF16 ? 2 : 4;

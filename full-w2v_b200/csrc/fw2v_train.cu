@@ -83,10 +83,14 @@ size_t launch_warp_smem(const TrainParams& p) {
   return train_smem_bytes(p.window, p.pitch, 1, s.r, p.prefetch != 0, p.bf16 ? 2 : 4);
 }
 
+// Static shared memory of the training kernel, with a margin: its parameter
+// block and the sigmoid table.
+size_t train_static_smem() { return sizeof(TrainParams) + kExpTableSize * sizeof(float) + 64; }
+
 // Whether one warp of a launch of p fits a block's shared memory (launch_t
 // takes 4, 2 or 1 warps per block, as many as fit).
 bool launch_fits(const TrainParams& p) {
-  return train_block_warps(launch_warp_smem(p), sizeof(TrainParams) + kExpTableSize * sizeof(float) + 64, 1) == 1;
+  return train_block_warps(launch_warp_smem(p), train_static_smem(), 1) == 1;
 }
 
 cudaError_t launch_train(const TrainParams& p, int num_sms, cudaStream_t st) {
