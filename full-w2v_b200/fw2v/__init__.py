@@ -456,6 +456,9 @@ class Batch:
         return v.value, n.value, s.value, p.value
 
     def set_launch(self, family: int, warps_per_block: int, blocks_per_sm: int = 0):
+        """Warps per block of a kernel family (1..8, 1..6, 1..4 for families
+        0, 1, 2; 0: the count that keeps the most warps resident) and a cap on
+        blocks per SM (0: as many as fit)."""
         self._check(lib().fw2v_batch_set_launch(self._h, family, warps_per_block, blocks_per_sm),
                     "batch_set_launch")
 
