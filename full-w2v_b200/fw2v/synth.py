@@ -86,38 +86,49 @@ def topic_tokens(n_tokens: int, vocab: int, topics: int, zipf_s: float, *, sente
     return out[:n_tokens], planted, purity
 
 
-def sbm_walks(nodes: int, blocks: int, degree: float, p_ratio: float, walks_per_node: int,
-              walk_len: int, *, seed: int = 0):
-    """Uniform random walks on a stochastic block model graph.
+def sbm_graph(nodes: int, blocks: int, degree: float, p_ratio: float, rng: np.random.Generator):
+    """A stochastic block model multigraph in CSR form.
 
-    Nodes are split into `blocks` equal blocks; edges inside a block are
-    p_ratio times as likely as edges across blocks, with `degree` expected
-    neighbours per node.  Returns (walks as an int32 [n_walks, walk_len] array
-    of node ids, block of each node).
+    Nodes are split into `blocks` equal blocks (node i in block
+    i * blocks // nodes); a node's expected degree is `degree`, and an edge
+    inside its block is p_ratio times as likely as one to any given node of
+    another block: p_in (bsize - 1) + p_out (nodes - bsize) = degree with
+    p_in = p_ratio p_out.  Edge counts are Poisson; an in-block edge joins a
+    uniform node and a uniform other node of its block, a cross-block edge a
+    uniform node and a uniform node of a uniform other block.  Returns
+    (offsets int64 [nodes + 1], neighbours int32, block of each node int32).
     """
-    rng = np.random.default_rng(seed)
     block = (np.arange(nodes) * blocks // nodes).astype(np.int32)
     bsize = nodes / blocks
-    # expected degree = p_in*(bsize-1) + p_out*(nodes-bsize), p_in = ratio*p_out
     p_out = degree / (p_ratio * (bsize - 1) + (nodes - bsize))
     n_in = rng.poisson(p_ratio * p_out * (bsize - 1) * nodes / 2)
-    n_out = rng.poisson(p_out * (nodes - bsize) * nodes / 2)
+    n_out = rng.poisson(p_out * (nodes - bsize) * nodes / 2) if blocks > 1 else 0
     a = rng.integers(0, nodes, n_in)
-    lo = (block[a] * nodes) // blocks
-    hi = ((block[a] + 1) * nodes) // blocks
-    b = lo + (rng.random(n_in) * (hi - lo)).astype(np.int64)
+    lo = (block[a].astype(np.int64) * nodes) // blocks
+    size = ((block[a].astype(np.int64) + 1) * nodes) // blocks - lo
+    b = lo + (a - lo + 1 + (rng.random(n_in) * (size - 1)).astype(np.int64)) % size
     c = rng.integers(0, nodes, n_out)
-    dd = rng.integers(0, nodes, n_out)
-    keep = block[c] != block[dd]
-    src = np.concatenate([a, b, c[keep], dd[keep]])
-    dst = np.concatenate([b, a, dd[keep], c[keep]])
-    ok = src != dst
+    other = (block[c].astype(np.int64) + 1 + rng.integers(0, max(blocks - 1, 1), n_out)) % blocks
+    lo2 = (other * nodes) // blocks
+    dd = lo2 + (rng.random(n_out) * (((other + 1) * nodes) // blocks - lo2)).astype(np.int64)
+    src = np.concatenate([a, b, c, dd])
+    dst = np.concatenate([b, a, dd, c])
+    ok = src != dst  # blocks of one node have no in-block partner
     src, dst = src[ok], dst[ok]
     order = np.argsort(src, kind="stable")
     src, dst = src[order], dst[order].astype(np.int32)
     offs = np.zeros(nodes + 1, np.int64)
     np.add.at(offs, src + 1, 1)
-    offs = np.cumsum(offs)
+    return np.cumsum(offs), dst, block
+
+
+def sbm_walks(nodes: int, blocks: int, degree: float, p_ratio: float, walks_per_node: int,
+              walk_len: int, *, seed: int = 0):
+    """Uniform random walks on a stochastic block model graph (sbm_graph).
+    Returns (walks as an int32 [n_walks, walk_len] array of node ids, block of
+    each node)."""
+    rng = np.random.default_rng(seed)
+    offs, dst, block = sbm_graph(nodes, blocks, degree, p_ratio, rng)
     deg = np.diff(offs)
     starts = np.repeat(np.arange(nodes, dtype=np.int32), walks_per_node)
     walks = np.empty((len(starts), walk_len), np.int32)
@@ -329,6 +340,40 @@ def make_topic_corpus_gpu(name: str, *, n_tokens: int | None = None, heldout_tok
     return corpus, held, cfg
 
 
+def sbm_graph_torch(nodes: int, blocks: int, degree: float, p_ratio: float, rng: np.random.Generator,
+                    gen, dev):
+    """sbm_graph() with torch on device `dev` (edge counts from the numpy
+    `rng`, endpoints from the torch generator `gen`): (offsets int64
+    [nodes + 1], neighbours int32, block of each node int64), as tensors."""
+    import torch
+    block = (torch.arange(nodes, device=dev, dtype=torch.int64) * blocks) // nodes
+    bsize = nodes / blocks
+    p_out = degree / (p_ratio * (bsize - 1) + (nodes - bsize))
+    n_in = int(rng.poisson(p_ratio * p_out * (bsize - 1) * nodes / 2))
+    n_out = int(rng.poisson(p_out * (nodes - bsize) * nodes / 2)) if blocks > 1 else 0
+    a = torch.randint(0, nodes, (n_in,), device=dev, generator=gen)
+    lo = (block[a] * nodes) // blocks
+    size = ((block[a] + 1) * nodes) // blocks - lo
+    u = torch.rand(n_in, device=dev, generator=gen, dtype=torch.float64)
+    b = lo + (a - lo + 1 + (u * (size - 1)).long()) % size
+    c = torch.randint(0, nodes, (n_out,), device=dev, generator=gen)
+    other = (block[c] + 1 + torch.randint(0, max(blocks - 1, 1), (n_out,), device=dev, generator=gen)) % blocks
+    lo2 = (other * nodes) // blocks
+    u2 = torch.rand(n_out, device=dev, generator=gen, dtype=torch.float64)
+    d = lo2 + (u2 * (((other + 1) * nodes) // blocks - lo2)).long()
+    src = torch.cat([a, b, c, d])
+    dst = torch.cat([b, a, d, c])
+    del a, b, c, d, lo, size, u, other, lo2, u2
+    ok = src != dst  # blocks of one node have no in-block partner
+    src, dst = src[ok], dst[ok]
+    order = torch.argsort(src, stable=True)
+    src, dst = src[order], dst[order].to(torch.int32).contiguous()
+    deg = torch.bincount(src, minlength=nodes)
+    offs = torch.zeros(nodes + 1, device=dev, dtype=torch.int64)
+    offs[1:] = torch.cumsum(deg, 0)
+    return offs, dst, block
+
+
 def sbm_corpus_gpu(nodes: int, blocks: int, degree: float, p_ratio: float, walks_per_node: int, walk_len: int, *,
                    seed: int = 0, device="cuda", min_count: int = 1, heldout_walks: int = 0):
     """sbm_walks() generated on a device, written as the reference's text
@@ -350,29 +395,7 @@ def sbm_corpus_gpu(nodes: int, blocks: int, degree: float, p_ratio: float, walks
     dev = torch.device(device)
     gen = torch.Generator(device=device)
     gen.manual_seed(seed)
-    block = (torch.arange(nodes, device=dev, dtype=torch.int64) * blocks) // nodes
-    bsize = nodes / blocks
-    p_out = degree / (p_ratio * (bsize - 1) + (nodes - bsize))
-    rng = np.random.default_rng(seed)
-    n_in = int(rng.poisson(p_ratio * p_out * (bsize - 1) * nodes / 2))
-    n_out = int(rng.poisson(p_out * (nodes - bsize) * nodes / 2))
-    a = torch.randint(0, nodes, (n_in,), device=dev, generator=gen)
-    lo = (block[a] * nodes) // blocks
-    hi = ((block[a] + 1) * nodes) // blocks
-    b = lo + (torch.rand(n_in, device=dev, generator=gen, dtype=torch.float64) * (hi - lo)).long()
-    c = torch.randint(0, nodes, (n_out,), device=dev, generator=gen)
-    d = torch.randint(0, nodes, (n_out,), device=dev, generator=gen)
-    keep = block[c] != block[d]
-    src = torch.cat([a, b, c[keep], d[keep]])
-    dst = torch.cat([b, a, d[keep], c[keep]])
-    ok = src != dst
-    src, dst = src[ok], dst[ok]
-    order = torch.argsort(src, stable=True)
-    src, dst = src[order], dst[order].to(torch.int32).contiguous()
-    deg = torch.bincount(src, minlength=nodes)
-    offs = torch.zeros(nodes + 1, device=dev, dtype=torch.int64)
-    offs[1:] = torch.cumsum(deg, 0)
-    del a, b, c, d, keep, ok, order, src
+    offs, dst, block = sbm_graph_torch(nodes, blocks, degree, p_ratio, np.random.default_rng(seed), gen, dev)
     cs = torch.cuda.current_stream(dev)
 
     def walks(starts, wseed):
