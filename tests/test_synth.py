@@ -143,3 +143,44 @@ def test_make_topic_corpus_at_config_size(name):
     assert corpus.counts[1:].sum() == cfg["n_tokens"]
     assert np.all(np.diff(corpus.counts[1:].astype(np.int64)) <= 0)
     assert np.all(np.diff(corpus.chunk_off) == 1000)
+
+
+def test_topic_corpus_on_the_device_generator_laws():
+    """The device generator (torch; run here on the CPU) at a small size."""
+    V, topics, n = 3000, 8, 300_000
+    corpus, held = synth.topic_corpus_gpu(n, V, topics, 1.0, min_count=1, seed=5, device="cpu",
+                                          heldout_tokens=20_000)
+    stream = corpus.stream.numpy()
+    assert stream[-1] == 0 and len(stream) == n + 1  # min_count 1 keeps every token
+    assert stream[:-1].min() >= 1 and stream[:-1].max() < len(corpus.counts)
+    assert np.array_equal(corpus.chunk_off.numpy(), np.arange(0, n, 1000))
+    counts = corpus.counts.astype(np.int64)
+    assert counts[0] == n // 1000 - 1 and np.all(np.diff(counts[1:]) <= 0)
+    assert np.array_equal(np.bincount(stream[:-1], minlength=len(counts))[1:], counts[1:])
+    # planted topics concentrate within a sentence (Dirichlet(0.1) weights)
+    lab = corpus.label[stream[:-1]].reshape(-1, 1000)
+    assert np.mean([np.bincount(r, minlength=topics).max() / 1000 for r in lab]) > 0.5
+    # Zipf(1) over affine permutations: the top word of each topic is its
+    # planted topic's word of rank 0, far above the median
+    assert counts[1] > 20 * counts[len(counts) // 2]
+    assert held is not None and len(held) <= 20_000 and held.min() >= 1
+
+
+def test_c3_corpus_keeps_every_word_at_sample_1e4():
+    """Subsampling never drops a word at the C3 shape: every word's expected
+    share of the corpus stays below the always-keep bound of the word2vec
+    rule, (sqrt(x) + 1) / x >= 1 for x = count / (sample * train_words) <=
+    ((1 + sqrt 5) / 2)^2 (improved_driver_functions.cpp:60-78)."""
+    c = synth.CONFIGS["c3"]
+    V, topics, s = c["vocab"], c["topics"], c["zipf_s"]
+    a, b = synth._affine_perms(V, topics, np.random.default_rng(1234 + 3))
+    p = np.arange(1, V + 1, dtype=np.float64) ** -s
+    p /= p.sum()
+    share = np.zeros(V)
+    words = np.arange(V, dtype=np.int64)
+    for z in range(topics):
+        rank = (pow(int(a[z]), -1, V) * ((words - b[z]) % V)) % V
+        share += p[rank]
+    share /= topics
+    bound = ((1 + 5 ** 0.5) / 2) ** 2 * c["sample"]
+    assert share.max() < 0.8 * bound
