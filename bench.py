@@ -104,14 +104,15 @@ class ClockSampler:
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 9:
                 continue
+            # a reason counts even in a sample whose clocks did not read
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
             try:
                 sm.append(float(parts[1]))
                 mx = float(parts[2])
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
         if not sm:
             return None
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
