@@ -32,7 +32,7 @@ def test_clock_summary_reads_median_clock_and_active_reasons():
         "0, [N/A], 1965, 1.0, 0x0, Not Active, Active, Not Active, Not Active",
     ]
     s = c.summary()
-    assert s == {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": ["hw_slowdown", "sw_power_cap"],
+    assert s == {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": ["hw_thermal_slowdown", "sw_power_cap"],
                  "samples": 3}
 
 
