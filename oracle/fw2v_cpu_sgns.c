@@ -123,20 +123,21 @@ static void* worker(void* arg) {
     for (int e = 0; e < sc->epochs && wk->rc == 0; e++) {
       int64_t ne = 0, nk = 0;
       uint64_t wr = 0;
-      wk->rc = orc_sample_epoch(sc, s, &st, cap, lens, alphas, cap, ids, negs, &ne, &nk, &wr);
+      /* a bounded sample samples only the sentences it trains */
+      if (wk->max_entries_per_stream > 0)
+        wk->rc = orc_sample_epoch_prefix(sc, s, &st, wk->max_entries_per_stream, cap, lens, alphas, cap, ids, negs,
+                                         &ne, &nk, &wr);
+      else
+        wk->rc = orc_sample_epoch(sc, s, &st, cap, lens, alphas, cap, ids, negs, &ne, &nk, &wr);
       if (wk->rc) break;
       int64_t off = 0;
-      int64_t lim = wk->max_entries_per_stream > 0 && wk->max_entries_per_stream < ne ? wk->max_entries_per_stream : ne;
-      uint64_t counted = 0;
-      for (int64_t i = 0; i < lim; i++) {
+      for (int64_t i = 0; i < ne; i++) {
         if (lens[i] > 0)
           train_sentence(tc, wk->syn0, wk->syn1, lens[i], ids + off, negs + off * K, alphas[i], cur, orig, o, o0);
         off += lens[i];
         wk->words_kept += (uint64_t)lens[i];
-        counted += (uint64_t)lens[i];
       }
-      /* words read scale with the share of kept words actually trained */
-      wk->words_read += lim == ne ? wr : (uint64_t)((double)wr * (double)counted / (double)(nk > 0 ? nk : 1));
+      wk->words_read += wr;
     }
     free(lens);
     free(alphas);
@@ -151,8 +152,9 @@ static void* worker(void* arg) {
 }
 
 /* Train `scfg->epochs` epochs of every stream on n_threads host threads.
- * max_entries_per_stream > 0 bounds the sentences trained per stream and epoch
- * (a sample of the workload); words_read is then scaled to the trained share. */
+ * max_entries_per_stream > 0 bounds the sentences sampled and trained per
+ * stream and epoch (a sample of the workload); words_read counts the tokens
+ * those sentences consumed. */
 int orc_cpu_sgns(const orc_sampler_cfg* scfg, const orc_train_cfg* tcfg, float* syn0, float* syn1neg,
                  int n_threads, int64_t max_entries_per_stream, uint64_t* words_read, uint64_t* words_kept) {
   if (n_threads < 1) n_threads = 1;

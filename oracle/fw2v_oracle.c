@@ -127,10 +127,12 @@ static void refresh_alpha(const orc_sampler_cfg* cfg, orc_stream_state* st) {
 }
 
 /* FULL-W2V-driver.cu:166-302 for one stream and one epoch. */
-int orc_sample_epoch(const orc_sampler_cfg* cfg, int stream_id, orc_stream_state* st,
-                     int64_t cap_entries, int32_t* lens, float* alphas, int64_t cap_kept,
-                     int32_t* ids, int32_t* negs, int64_t* n_entries, int64_t* n_kept,
-                     uint64_t* words_read) {
+/* One epoch of a stream, or its first stop_after entries (stop_after > 0):
+ * the entries are the same as the full epoch's first ones and *words_read
+ * counts the tokens those entries consumed. */
+static int sample_epoch(const orc_sampler_cfg* cfg, int stream_id, orc_stream_state* st, int64_t stop_after,
+                        int64_t cap_entries, int32_t* lens, float* alphas, int64_t cap_kept, int32_t* ids,
+                        int32_t* negs, int64_t* n_entries, int64_t* n_kept, uint64_t* words_read) {
   int64_t es, ee;
   orc_stream_range(cfg, stream_id, &es, &ee);
   const int K = cfg->negative;
@@ -187,11 +189,28 @@ int orc_sample_epoch(const orc_sampler_cfg* cfg, int stream_id, orc_stream_state
     alphas[ne] = st->alpha;
     ne++;
     nk += L;
+    if (stop_after > 0 && ne >= stop_after) break;
   }
   *n_entries = ne;
   *n_kept = nk;
   *words_read = word_count;
   return 0;
+}
+
+int orc_sample_epoch(const orc_sampler_cfg* cfg, int stream_id, orc_stream_state* st,
+                     int64_t cap_entries, int32_t* lens, float* alphas, int64_t cap_kept,
+                     int32_t* ids, int32_t* negs, int64_t* n_entries, int64_t* n_kept,
+                     uint64_t* words_read) {
+  return sample_epoch(cfg, stream_id, st, 0, cap_entries, lens, alphas, cap_kept, ids, negs, n_entries, n_kept,
+                      words_read);
+}
+
+int orc_sample_epoch_prefix(const orc_sampler_cfg* cfg, int stream_id, orc_stream_state* st,
+                            int64_t max_entries, int64_t cap_entries, int32_t* lens, float* alphas,
+                            int64_t cap_kept, int32_t* ids, int32_t* negs, int64_t* n_entries,
+                            int64_t* n_kept, uint64_t* words_read) {
+  return sample_epoch(cfg, stream_id, st, max_entries > 0 ? max_entries : 1, cap_entries, lens, alphas, cap_kept,
+                      ids, negs, n_entries, n_kept, words_read);
 }
 
 /* ---------------- SGNS update ---------------- */

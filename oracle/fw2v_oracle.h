@@ -96,6 +96,14 @@ int orc_sample_epoch(const orc_sampler_cfg* cfg, int stream_id, orc_stream_state
                      int32_t* ids, int32_t* negs, int64_t* n_entries, int64_t* n_kept,
                      uint64_t* words_read);
 
+/* The first max_entries entries of that epoch (fewer if it ends before), with
+ * *words_read the tokens they consumed: a bounded sample of the workload.  The
+ * stream state is left mid-epoch. */
+int orc_sample_epoch_prefix(const orc_sampler_cfg* cfg, int stream_id, orc_stream_state* st,
+                            int64_t max_entries, int64_t cap_entries, int32_t* lens, float* alphas,
+                            int64_t cap_kept, int32_t* ids, int32_t* negs, int64_t* n_entries,
+                            int64_t* n_kept, uint64_t* words_read);
+
 /* ---- SGNS update (FULL-W2V-kernels.cu:106-250, textbook windows) ---- */
 enum { ORC_F64 = 64, ORC_F32 = 32 };
 enum { ORC_SIGMOID_TABLE = 0, ORC_SIGMOID_EXACT = 1 };

@@ -76,6 +76,11 @@ def _declare(L):
                                    C.c_int64, P, P, C.c_int64, P, P,
                                    C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                    C.POINTER(C.c_uint64)]
+    L.orc_sample_epoch_prefix.restype = C.c_int
+    L.orc_sample_epoch_prefix.argtypes = [C.POINTER(SamplerCfg), C.c_int, C.POINTER(StreamState), C.c_int64,
+                                          C.c_int64, P, P, C.c_int64, P, P,
+                                          C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                          C.POINTER(C.c_uint64)]
     for name in ("orc_train_f32", "orc_train_f64"):
         f = getattr(L, name)
         f.restype = C.c_int
@@ -212,6 +217,39 @@ def sample_streams(corpus: Corpus, *, threads: int, msl: int, negative: int, epo
                                          negs[: k * negative].copy(), int(wr.value)))
         out.append(per_epoch)
     return out
+
+
+def sample_stream_prefix(corpus: Corpus, stream_id: int, max_entries: int, *, threads: int, msl: int,
+                         negative: int, alpha0: float, sample: float, table_size: int = UNIGRAM_TABLE_SIZE,
+                         epochs: int = 1) -> StreamEpoch:
+    """The first max_entries batch entries of stream stream_id's first epoch
+    (orc_sample_epoch_prefix, the CPU baseline's bounded sample), with the
+    tokens they consumed."""
+    L = lib()
+    stream = np.ascontiguousarray(corpus.stream, np.int32)
+    chunk_off = np.ascontiguousarray(corpus.chunk_off, np.int64)
+    counts = np.ascontiguousarray(corpus.counts, np.uint32)
+    p_keep = subsample_table(counts, sample, corpus.train_words) if sample > 0 else \
+        np.zeros(len(counts), np.float32)
+    rs, rw = unigram_runs(counts, table_size)
+    cfg = SamplerCfg(_p(stream).value, len(stream), _p(chunk_off).value, len(chunk_off), _p(p_keep).value, sample,
+                     _p(rs).value, _p(rw).value, len(rw), table_size, threads, msl, negative, epochs, alpha0,
+                     corpus.train_words)
+    st = StreamState()
+    L.orc_stream_init(C.byref(cfg), stream_id, C.byref(st))
+    cap = len(stream) + 2
+    lens = np.zeros(cap, np.int32)
+    alphas = np.zeros(cap, np.float32)
+    ids = np.zeros(cap, np.int32)
+    negs = np.zeros(cap * max(negative, 1), np.int32)
+    ne, nk, wr = C.c_int64(), C.c_int64(), C.c_uint64()
+    rc = L.orc_sample_epoch_prefix(C.byref(cfg), stream_id, C.byref(st), max_entries, cap, _p(lens), _p(alphas),
+                                   cap, _p(ids), _p(negs), C.byref(ne), C.byref(nk), C.byref(wr))
+    if rc != 0:
+        raise RuntimeError(f"orc_sample_epoch_prefix failed: {rc}")
+    n, k = ne.value, nk.value
+    return StreamEpoch(lens[:n].copy(), alphas[:n].copy(), ids[:k].copy(), negs[: k * negative].copy(),
+                       int(wr.value))
 
 
 def libc_shuffle(chunk_off: np.ndarray) -> np.ndarray:
