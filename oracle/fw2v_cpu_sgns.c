@@ -7,9 +7,9 @@
  * each sentence with the oracle's batch builder and trains it at once with the
  * FULL-W2V method (per-position context copies reused for the whole window
  * lifetime, one fresh read and one write-back per target row) on tables shared
- * by all threads without locks (Hogwild, like word2vec).  FP32, plain
- * sequential dot products with eight partial sums so the compiler can
- * vectorise them.  The product never calls this file.
+ * by all threads without locks (Hogwild, like word2vec).  FP32, dot products
+ * with eight partial sums and elementwise loops that the compiler vectorises.
+ * The product never calls this file.
  */
 #include <math.h>
 #include <pthread.h>
@@ -29,7 +29,15 @@ typedef struct {
   int rc;
 } worker_t;
 
-static float dot8(const float* a, const float* b, int d) {
+/* The hot loops are compiled for AVX-512, AVX2 + FMA and the baseline ISA,
+ * and the loader picks the widest the host supports (GCC function clones). */
+#if defined(__x86_64__) && defined(__GNUC__) && !defined(__clang__)
+#define HOT __attribute__((target_clones("arch=skylake-avx512", "arch=haswell", "default")))
+#else
+#define HOT
+#endif
+
+HOT static float dot8(const float* restrict a, const float* restrict b, int d) {
   float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int e = 0;
   for (; e + 8 <= d; e += 8)
@@ -37,6 +45,20 @@ static float dot8(const float* a, const float* b, int d) {
   float t = ((s[0] + s[4]) + (s[1] + s[5])) + ((s[2] + s[6]) + (s[3] + s[7]));
   for (; e < d; e++) t += a[e] * b[e];
   return t;
+}
+
+/* v += g*o and o += g*v_old */
+HOT static void update2(float* restrict v, float* restrict o, float g, int d) {
+  for (int e = 0; e < d; e++) {
+    const float vo = v[e];
+    v[e] = vo + g * o[e];
+    o[e] += g * vo;
+  }
+}
+
+/* row += a - b */
+HOT static void add_delta(float* restrict row, const float* restrict a, const float* restrict b, int d) {
+  for (int e = 0; e < d; e++) row[e] += a[e] - b[e];
 }
 
 static float grad(const orc_train_cfg* c, float x, int label, float alpha) {
@@ -74,19 +96,14 @@ static void train_sentence(const orc_train_cfg* c, float* syn0, float* syn1, int
         for (int j = 0; j < n; j++) {
           float* v = cur + (int64_t)ctx[j] * d;
           float g = grad(c, dot8(v, o, d), k == 0, alpha);
-          for (int e = 0; e < d; e++) {
-            float vo = v[e];
-            v[e] = vo + g * o[e];
-            o[e] += g * vo;
-          }
+          update2(v, o, g, d);
         }
-        for (int e = 0; e < d; e++) row[e] += o[e] - o0[e];
+        add_delta(row, o, o0, d);
       }
     }
     if (w - W >= 0) {
       int p = w - W;
-      float* row = syn0 + (int64_t)ids[p] * P;
-      for (int e = 0; e < d; e++) row[e] += cur[(int64_t)p * d + e] - orig[(int64_t)p * d + e];
+      add_delta(syn0 + (int64_t)ids[p] * P, cur + (int64_t)p * d, orig + (int64_t)p * d, d);
     }
     if (w + W + 1 < L) {
       int p = w + W + 1;
@@ -94,10 +111,8 @@ static void train_sentence(const orc_train_cfg* c, float* syn0, float* syn1, int
       memcpy(orig + (int64_t)p * d, cur + (int64_t)p * d, sizeof(float) * d);
     }
   }
-  for (int p = L - W > 0 ? L - W : 0; p < L; p++) {
-    float* row = syn0 + (int64_t)ids[p] * P;
-    for (int e = 0; e < d; e++) row[e] += cur[(int64_t)p * d + e] - orig[(int64_t)p * d + e];
-  }
+  for (int p = L - W > 0 ? L - W : 0; p < L; p++)
+    add_delta(syn0 + (int64_t)ids[p] * P, cur + (int64_t)p * d, orig + (int64_t)p * d, d);
 }
 
 static void* worker(void* arg) {
